@@ -1,0 +1,208 @@
+/*
+ * msg123_gpu.h -- C ABI of the B200 Newton-Krylov library for the 3D Richards
+ * equation (drop-in for Msg123's Nonlinear_solution / Linear_solution path).
+ *
+ * All entry points take plain host pointers and sizes.  The library copies the
+ * inputs to device memory, owns every device allocation, and returns an int
+ * status: 0 = ok, >0 = soft failure (no convergence), <0 = hard error (message
+ * in msg_gpu_last_error()).  No exception ever crosses the ABI.  One context
+ * per host thread.
+ *
+ * Units follow the reference after nondimensionalisation: every length is
+ * divided by len_scal (reference Read_input.f90:1100-1112), alpha and Ss are
+ * multiplied by it and Ks is divided by it (Assign_calculation.f90:117,259-260).
+ * Cell numbering is the reference local order: x fastest, then y, then layers
+ * from the top down (Set_cell.f90:845-925).  Face order is
+ * up(1) north(2) west(3) east(4) south(5) down(6) (Set_condition.f90:1584-2026).
+ */
+#ifndef MSG123_GPU_H
+#define MSG123_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MSG_API __attribute__((visibility("default")))
+#else
+#define MSG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (Newton / Krylov / time loop outcome). */
+enum {
+  MSG_OK = 0,
+  MSG_NEWTON_MAXIT = 1,      /* out_iter reached maxout_iter      (Nonlinear_solution.f90:278-282) */
+  MSG_NAN = 2,               /* NaN in the update                  (Nonlinear_solution.f90:151-155) */
+  MSG_LINESEARCH_FAIL = 3,   /* back_flag set by run_backtr        (Nonlinear_solution.f90:265-269) */
+  MSG_DIVERGED = 4,          /* |dh| >= VARMAX or |h| >= XMAX       (Nonlinear_solution.f90:283-287) */
+  MSG_DT_TOO_SMALL = 5,      /* delt < DSMAL                        (Time_module.f90:72-73) */
+  MSG_ERR_ARG = -1,
+  MSG_ERR_CUDA = -2,
+  MSG_ERR_SIZE = -3,
+  MSG_ERR_STATE = -4
+};
+
+/* Problem description: what set_cell_info / make_cell / set_connect consume.
+ * Arrays are host pointers, read only during msg_gpu_create. */
+typedef struct msg_grid {
+  int32_t nx, ny, nz;        /* active box; ncalc = nx*ny*nz, ncals = nx*ny (top layer) */
+  int32_t sea_top;           /* 1: a fixed-head ("sea") layer sits above the top layer   */
+  int32_t free_drainage;     /* 1: unit-gradient outflow through the bottom face (extension, no reference counterpart) */
+  int32_t pad0;
+  const float *reta, *retn, *resi, *poro, *ss;  /* [ncalc] real(SP) soil parameters (Assign_calculation.f90:19-21) */
+  const float *ksx, *ksy, *ksz;                  /* [ncalc] real(SP) saturated conductivity                */
+  const double *cell_top, *cell_vol;             /* [ncalc] (Make_cell.f90:11-13)                          */
+  const double *dis2face;    /* [6*ncalc] centre-to-face distance, face-major: [f*ncalc + i]               */
+  const double *face_area;   /* [6*ncalc] face areas, face-major                                           */
+  const double *area_r;      /* [ncals] plan area that receives recharge (rech_area)                       */
+  const double *surf_top, *surf_bott, *surf_reli, *surf_parm;  /* [ncals] surface term (Prep_calculation.f90:173-201) */
+  const double *sea_head;    /* [ncals] fixed head of the sea cell above each top cell (read_seal)          */
+} msg_grid_t;
+
+/* Solver knobs: the namelist set_solution / set_amg (Initial_module.f90:355-359)
+ * plus the extensions the synthetic configurations need. */
+typedef struct msg_params {
+  double len_scal;           /* real(SP) len_scal promoted to double                                 */
+  double criteria;           /* Newton criterion on max|dh|*len_scal (Nonlinear_solution.f90:144-150) */
+  double lin_tol;            /* >0: fixed BiCGStab tolerance; 0: Eisenstat-Walker eta (reference)     */
+  int32_t criteria_rel;      /* 1: criteria is multiplied by max|h|*len_scal (relative head tolerance) */
+  int32_t maxout_iter;       /* Newton iteration cap                                                  */
+  int32_t maxinn_iter;       /* BiCGStab iteration cap                                                */
+  int32_t precon_type;       /* 0: DILU / ILU(0); 1: AMG                                              */
+  int32_t ref_quirks;        /* 1: AMG preconditioner reproduces the reference (output = fine DILU)    */
+  int32_t precision;         /* 0: FP64 everywhere; 1: FP32 V-cycle, BF16 coarse operators            */
+  int32_t amg_nlevel;        /* maximum number of AMG levels                                          */
+  int32_t amg_coarse_max;    /* coarsest level is solved directly once it has <= this many rows       */
+  int32_t amg_sweeps;        /* Jacobi sweeps before and after the coarse correction                  */
+  float jac_omega;           /* prolongation smoothing weight (real(SP))                               */
+  float amg_theta;           /* strength threshold (real(SP))                                          */
+  float smooth_omega;        /* Jacobi smoother weight                                                */
+  int32_t sim_type;          /* 0: delt*inc_fact per accepted step; 1: heuristic (apply_heuri)         */
+  int32_t pad1;
+  double ini_step;           /* initial delt (s)                                                      */
+  double inc_fact;           /* factor for sim_type 0                                                 */
+  double max_step;           /* cap on delt for sim_type 1                                            */
+  double end_time;           /* simulation end (s)                                                    */
+} msg_params_t;
+
+/* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */
+typedef struct msg_stats {
+  int32_t status;            /* MSG_OK when converged                                 */
+  int32_t out_iter;          /* Newton iterations                                     */
+  int32_t inner_total;       /* BiCGStab iterations summed over the Newton iterations */
+  int32_t back_total;        /* backtracking steps summed                             */
+  int32_t in_iter_last, back_iter_last;
+  int32_t maxnun;            /* 1-based cell of the largest change (last iteration)   */
+  int32_t pad;
+  double maxvar;             /* signed largest change * len_scal                      */
+  double l2_new;             /* ||F(h)||^2 at exit                                    */
+} msg_stats_t;
+
+/* Time loop statistics. */
+typedef struct msg_run_stats {
+  int32_t status;
+  int32_t accepted;          /* accepted time steps                      */
+  int32_t rejected;          /* rejected attempts (dt halved)             */
+  int32_t newton_total;      /* Newton iterations over accepted + rejected */
+  int32_t krylov_total;
+  int32_t back_total;
+  double current_t;          /* simulated time reached (s)               */
+  double delt;               /* delt after the last step                  */
+} msg_run_stats_t;
+
+typedef struct msg_ctx msg_ctx_t;
+
+/* Last error message of this thread. */
+MSG_API const char *msg_gpu_last_error(void);
+
+/* Allocate a context on the current CUDA device and build the connectivity on
+ * the GPU.  Replaces allocate_solvar + set_connect (Allocate_solution.f90:56-197,
+ * Set_condition.f90:1584-2158) and prepare_calc's newper (Prep_calculation.f90:79). */
+MSG_API int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t **out);
+MSG_API void msg_gpu_destroy(msg_ctx_t *ctx);
+
+/* Export the reference CSR built on the GPU (off_index, off_row 1-based, conn_dir,
+ * left_off, right_off, sat_hydf, area_dis; Set_condition.f90:1584-2026).  Each
+ * pointer may be NULL.  nnz receives off_index(ncalc). */
+MSG_API int msg_gpu_get_connect(msg_ctx_t *ctx, int32_t *offind, int32_t *offrow, int32_t *conn_dir,
+                        int32_t *left_off, int32_t *right_off, double *hydf_conn,
+                        double *abyd_conn, int32_t *nnz);
+
+/* Set the time-level state (head_new, head_old, srat_old, surf_head, surf_old)
+ * and delt.  NULL leaves a field unchanged. */
+MSG_API int msg_gpu_set_state(msg_ctx_t *ctx, const double *head_new, const double *head_old,
+                      const double *srat_old, const double *surf_head, double delt);
+MSG_API int msg_gpu_get_state(msg_ctx_t *ctx, double *head_new, double *head_old, double *srat_new,
+                      double *srat_old, double *surf_head);
+
+/* t = 0 branch of calc_nextst (Time_module.f90:142-196): head_new = head_old = head,
+ * srat_old = srat_new = calc_srat_rperm(head), surf_head = surf_old = head (top layer). */
+MSG_API int msg_gpu_init_state(msg_ctx_t *ctx, const double *head, double delt);
+
+/* Recharge volume rate per surface cell (calc_rech, Time_module.f90:88-94). */
+MSG_API int msg_gpu_set_recharge(msg_ctx_t *ctx, const double *calc_rech);
+
+/* calc_srat_rperm (Calc_parameter.f90:15-77) on a host head vector. */
+MSG_API int msg_gpu_srat_rperm(msg_ctx_t *ctx, const double *pres, double pertur, double *srat,
+                       double *rperm, double *sstor);
+
+/* calc_func (Calc_function.f90:24-101): funcv = F(infx). */
+MSG_API int msg_gpu_calc_func(msg_ctx_t *ctx, const double *infx, double *funcv);
+
+/* make_matvec (Make_linearsystem.f90:24-68) at the current head_new: the Jacobian
+ * diagonal dmat[ncalc], off-diagonals lumat[nnz] in the reference CSR order and
+ * rhs = -F.  Any output may be NULL; the system stays on the device for the
+ * next msg_gpu_solve_linalg. */
+MSG_API int msg_gpu_make_matvec(msg_ctx_t *ctx, double *dmat, double *lumat, double *rhs);
+
+/* Load a level-1 system array_var(1)%{dmat,lumat,rhs} (lumat in reference CSR order)
+ * as make_matvec would leave it, and build the AMG hierarchy when precon_type = 1. */
+MSG_API int msg_gpu_set_system(msg_ctx_t *ctx, const double *dmat, const double *lumat, const double *rhs);
+
+/* Apply the preconditioner of the current system once: z = M^-1 r (solve_ilu with the
+ * DILU diagonal, Linear_solution.f90:742-855, or one AMG V-cycle). */
+MSG_API int msg_gpu_precond(msg_ctx_t *ctx, const double *r, double *z);
+
+/* calc_vecjacf (Calc_function.f90:515-621): out = J(x) v by Brown-Saad differencing. */
+MSG_API int msg_gpu_vecjacf(msg_ctx_t *ctx, const double *x, const double *v, double *out);
+
+/* solve_linalg (Linear_solution.f90:26-58): BiCGStab on the system of the last
+ * make_matvec with bnorm = init_norm and tolerance errtol, starting from inx. */
+MSG_API int msg_gpu_solve_linalg(msg_ctx_t *ctx, double init_norm, double errtol, double *inx,
+                         double *last_norm, int32_t *in_iter, int32_t *conv_flag);
+
+/* calc_numsol (Nonlinear_solution.f90:33-294): one time level's Newton solve. */
+MSG_API int msg_gpu_calc_numsol(msg_ctx_t *ctx, msg_stats_t *stats);
+
+/* Time loop (Msg.f90:83-104 with update_tstep/calc_nextst, Time_module.f90:34-273):
+ * advance until nsteps more steps are accepted or end_time is reached.
+ * rech_until/rech_after: the recharge array applies until simulated time
+ * rech_until (s), after which it is scaled by rech_after (0 = rain stops). */
+MSG_API int msg_gpu_advance(msg_ctx_t *ctx, int32_t nsteps, double rech_until, double rech_after,
+                    msg_run_stats_t *stats);
+
+/* calc_mass (Calc_function.f90:103-174) summed over cells: out[0..7] =
+ * storage, flow, recharge, well, surface, river, lake, sea (+ out[8] drainage),
+ * each a volume over the step (rate * delt). */
+MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
+
+/* Device time spent in the last advance/numsol call split by phase (ms):
+ * [0] assembly, [1] Krylov, [2] AMG setup, [3] residual evaluations, [4] total. */
+MSG_API int msg_gpu_timers(msg_ctx_t *ctx, double *ms5);
+/* Time `reps` back-to-back launches of one kernel class on the context's stream with
+ * CUDA events, inputs = the current state: 0 = stencil SpMV (FP64), 1 = calc_func,
+ * 2 = make_matvec, 3 = one preconditioner apply, 4 = AMG setup.  Result in ms per launch. */
+MSG_API int msg_gpu_kernel_time(msg_ctx_t *ctx, int32_t which, int32_t reps, double *ms_per_launch);
+
+/* Number of kernels this library has launched in this process (all contexts). */
+MSG_API long long msg_gpu_launch_count(void);
+
+/* Enable (1) or disable (0) the per-phase CUDA-event timers (adds syncs). */
+MSG_API int msg_gpu_set_timing(msg_ctx_t *ctx, int32_t on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSG123_GPU_H */

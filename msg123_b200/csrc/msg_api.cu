@@ -1,0 +1,751 @@
+// msg_api.cu -- C ABI of libmsg123gpu.so: context lifecycle, state transfer, and the
+// host-side control of the Newton iteration (calc_numsol) and of the time loop.
+//
+// The control flow restates Nonlinear_solution.f90 and Time_module.f90; every
+// vector operation runs on the device and only scalars (norms, dot products, the
+// arg-max of the update) cross PCIe.
+#include "msg_ctx.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace msg {
+
+static thread_local char g_err[512] = "";
+long long g_launches = 0;
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+const char *get_error() { return g_err; }
+
+static constexpr double VARMAX = 1.0e3, XMAX = 1.0e4, DSMAL = 1.0e-20;
+static constexpr double MACHI_EPS = 1.1920928955078125e-07;   // epsilon(1._SP)
+
+static int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
+__global__ void k_fill(int n, double *y, double v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = v;
+}
+__global__ void k_scale_copy(int n, double *y, const double *x, double a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = __dmul_rn(x[i], a);
+}
+// outjvec = -(f2 - f1) * eps_inv  (calc_vecjacf, Calc_function.f90:613-617)
+__global__ void k_vecjac_out(int n, double *out, const double *f2, const double *f1, double eps_inv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = __dmul_rn(-__dsub_rn(f2[i], f1[i]), eps_inv);
+}
+__global__ void k_csr_to_dia(int nx, int ny, int nz, const int *offind, const double *lumat, double *lu) {
+  int N = nx * ny * nz, nxy = nx * ny;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int iz = i / nxy, rem = i - iz * nxy, iy = rem / nx, ix = rem - iy * nx;
+  const bool has[6] = {iz > 0, iy > 0, ix > 0, ix < nx - 1, iy < ny - 1, iz < nz - 1};
+  int k = offind[i];
+  for (int d = 0; d < 6; ++d) lu[(size_t)d * N + i] = has[d] ? lumat[k++] : 0.0;
+}
+
+static double sum_part(msg_ctx *c, int count, int *rc) {
+  *rc = MSG_OK;
+  cudaError_t e = cudaMemcpyAsync(c->hpin, c->part, (size_t)count * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { set_error("partials: %s", cudaGetErrorString(e)); *rc = MSG_ERR_CUDA; return 0.0; }
+  double s = 0.0;
+  for (int b = 0; b < count; ++b) s += c->hpin[b];
+  return s;
+}
+
+// calc_func + its squared norm
+static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
+  int rc = launch_calc_func(c, h, F, true);
+  if (rc) return rc;
+  *l2 = sum_part(c, nblk(c->N), &rc);
+  return rc;
+}
+
+// make_matvec (Make_linearsystem.f90:24-68) + AMG setup when requested.
+static int make_matvec(msg_ctx *c, double *l2_rhs) {
+  cudaEvent_t *ev = c->ev;
+  if (c->timing) cudaEventRecord(ev[0], c->stream);
+  int rc = launch_make_matvec(c);
+  if (rc) return rc;
+  double s = sum_part(c, nblk(c->N), &rc);
+  if (rc) return rc;
+  if (l2_rhs) *l2_rhs = s;
+  if (c->timing) cudaEventRecord(ev[1], c->stream);
+  if (c->prm.precon_type == 1 && !c->prm.ref_quirks) {
+    if ((rc = amg_setup(c))) return rc;
+  }
+  if (c->timing) {
+    cudaEventRecord(ev[2], c->stream);
+    cudaEventSynchronize(ev[2]);
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    c->t_ms[0] += a; c->t_ms[2] += b;
+  }
+  return MSG_OK;
+}
+
+static int solve_linalg(msg_ctx *c, double init_norm, double *x, double *last_norm) {
+  if (c->timing) cudaEventRecord(c->ev[3], c->stream);
+  c->bnorm = init_norm;
+  int rc = solve_bicgs(c, x);
+  if (rc) return rc;
+  *last_norm = c->rnorm;
+  if (c->timing) {
+    cudaEventRecord(c->ev[4], c->stream);
+    cudaEventSynchronize(c->ev[4]);
+    float a = 0.f;
+    cudaEventElapsedTime(&a, c->ev[3], c->ev[4]);
+    c->t_ms[1] += a;
+  }
+  return MSG_OK;
+}
+
+// calc_vecjacf (Calc_function.f90:515-621)
+static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out) {
+  const int n = c->N;
+  double *f1 = c->v, *f2 = c->t, *jc = c->z;
+  int rc;
+  double dummy;
+  if ((rc = func_norm(c, x, f1, &dummy))) return rc;
+  double l2_v, l2_x, l1_v;
+  if ((rc = dot(c, v, v, n, &l2_v))) return rc;
+  if ((rc = dot(c, x, v, n, &l2_x))) return rc;
+  if ((rc = norm1(c, v, n, &l1_v))) return rc;
+  double sign = (l2_x < 0.0) ? -1.0 : 1.0;
+  double eps = sign * std::sqrt(MACHI_EPS) * std::fmax(std::fabs(l2_x), l1_v) / l2_v;
+  double eps_inv = 1.0 / eps;
+  if ((rc = axpby(c, jc, x, eps, v, n))) return rc;
+  if ((rc = func_norm(c, jc, f2, &dummy))) return rc;
+  k_vecjac_out<<<kRedBlocks, 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
+  MSG_CHECK_LAUNCH();
+  return MSG_OK;
+}
+
+static int calc_funcl2norm(msg_ctx *c, double in_lam) {
+  int rc = axpby(c, c->head_new, c->head_pre, in_lam, c->head_change, c->N);
+  if (rc) return rc;
+  return func_norm(c, c->head_new, c->new_f, &c->l2_new);
+}
+
+// run_backtr (Nonlinear_solution.f90:441-631)
+static int run_backtr(msg_ctx *c) {
+  const int n = c->N;
+  const double back_alpha = 1.0e-4, back_beta = 0.9;
+  double l2_new2 = c->l2_new, lam2 = 1.0, maxpnorm = 1.0, lam_len = 1.0;
+  double temp_lam, rhs1, rhs2, lam_inv, lam2_inv, del_lam, av, bv, root, lam_max, lam_base, lam_diff, lam_incr;
+  int rc;
+  c->lam = 1.0;
+  double dummy;
+  if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
+  double l2_pnorm;
+  if ((rc = dot(c, c->head_change, c->head_change, n, &l2_pnorm))) return rc;
+  double *jacvec = c->tmpv;
+  if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec))) return rc;
+  double sql2_pnorm = std::sqrt(l2_pnorm);
+  if (sql2_pnorm > c->maxstep) {
+    maxpnorm = c->maxstep / sql2_pnorm;
+    if ((rc = scale(c, c->head_change, maxpnorm, n))) return rc;
+    sql2_pnorm = c->maxstep;
+  }
+  double step_len = sql2_pnorm;
+  if ((rc = dot(c, c->new_f, c->new_f, n, &c->l2_new))) return rc;
+  double slope;
+  if ((rc = dot(c, c->slope_rhs, jacvec, n, &slope))) return rc;
+  slope = slope * maxpnorm;
+  if ((rc = lam_length(c, c->head_change, c->head_new, &lam_len))) return rc;
+  c->l2_jnorm = c->l2_jnorm * maxpnorm * maxpnorm;
+  double step_tol = std::pow(MACHI_EPS, 2.0 / 3.0);
+  double lam_min = step_tol / lam_len;
+  double alpha_cond = 0.5 * c->l2_pre + back_alpha * c->lam * slope, beta_cond;
+  c->gradient = slope;
+  for (;;) {
+    if (0.5 * c->l2_new <= alpha_cond) break;
+    c->back_iter++;
+    if ((rc = calc_funcl2norm(c, c->lam))) return rc;
+    if (c->lam == 1.0) {
+      temp_lam = -slope / (2.0 * (0.5 * c->l2_new - 0.5 * c->l2_pre - slope));
+    } else {
+      rhs1 = 0.5 * c->l2_new - 0.5 * c->l2_pre - c->lam * slope;
+      rhs2 = l2_new2 - 0.5 * c->l2_pre - lam2 * slope;
+      lam_inv = 1.0 / (c->lam * c->lam);
+      lam2_inv = 1.0 / (lam2 * lam2);
+      del_lam = 1.0 / (c->lam - lam2);
+      av = (rhs1 * lam_inv - rhs2 * lam2_inv) * del_lam;
+      bv = (-lam2 * rhs1 * lam_inv + c->lam * rhs2 * lam2_inv) * del_lam;
+      if (av == 0) {
+        temp_lam = -slope / (2.0 * bv);
+      } else {
+        root = bv * bv - 3.0 * av * slope;
+        if (root < 0.0) temp_lam = 0.5 * c->lam;
+        else if (bv <= 0.0) temp_lam = (-bv + std::sqrt(root)) / (3.0 * av);
+        else temp_lam = -slope / (bv + std::sqrt(root));
+        if (temp_lam > 0.5 * c->lam) temp_lam = 0.5 * c->lam;
+      }
+    }
+    lam2 = c->lam;
+    l2_new2 = 0.5 * c->l2_new;
+    c->lam = std::fmax(temp_lam, 0.1 * c->lam);
+    if (c->lam < lam_min) { c->back_flag = 1; return MSG_OK; }
+    alpha_cond = 0.5 * c->l2_pre + back_alpha * c->lam * slope;
+  }
+  alpha_cond = 0.5 * c->l2_pre + back_alpha * c->lam * slope;
+  beta_cond = 0.5 * c->l2_pre + back_beta * c->lam * slope;
+  if (0.5 * c->l2_new < beta_cond) {
+    if (c->lam == 1.0 && sql2_pnorm < step_len) {
+      lam_max = step_len / sql2_pnorm;
+      for (;;) {
+        if (0.5 * c->l2_new > alpha_cond || 0.5 * c->l2_new >= beta_cond || c->lam >= lam_max) break;
+        lam2 = c->lam; l2_new2 = 0.5 * c->l2_new; c->lam = std::fmin(2.0 * c->lam, lam_max);
+        if ((rc = calc_funcl2norm(c, c->lam))) return rc;
+        alpha_cond = 0.5 * c->l2_pre + back_alpha * c->lam * slope;
+        beta_cond = 0.5 * c->l2_pre + back_beta * c->lam * slope;
+      }
+    }
+    if (c->lam < 1.0 || (c->lam > 1.0 && 0.5 * c->l2_new > alpha_cond)) {
+      lam_base = std::fmin(c->lam, lam2);
+      lam_diff = std::fabs(lam2 - c->lam);
+      for (;;) {
+        if (0.5 * c->l2_new <= alpha_cond && (0.5 * c->l2_new >= beta_cond || lam_diff <= lam_min)) break;
+        lam_incr = 0.5 * lam_diff;
+        c->lam = lam_base + lam_incr;
+        if ((rc = calc_funcl2norm(c, c->lam))) return rc;
+        alpha_cond = 0.5 * c->l2_pre + back_alpha * c->lam * slope;
+        beta_cond = 0.5 * c->l2_pre + back_beta * c->lam * slope;
+        if (0.5 * c->l2_new > alpha_cond) lam_diff = lam_incr;
+        else if (0.5 * c->l2_new < beta_cond) { lam_base = c->lam; lam_diff = lam_diff - lam_incr; }
+        if (lam_diff == 0.0) break;
+      }
+      if (0.5 * c->l2_new < beta_cond) {
+        if ((rc = calc_funcl2norm(c, lam_base))) return rc;
+        c->beta_iter++;
+      }
+      if (c->beta_iter == 10) { c->back_flag = 1; return MSG_OK; }
+    }
+  }
+  (void)l2_new2;
+  return MSG_OK;
+}
+
+// set_eater (Nonlinear_solution.f90:414-439)
+static void set_eater(msg_ctx *c) {
+  const double eta_max = 0.9, eta_min = 1.0e-4, eta_alpha = (1.0 + std::sqrt(5.0)) / 2.0;
+  double eta_safe = std::pow(c->eta, eta_alpha);
+  double minus1 = 1.0 - c->lam;
+  double lin = std::sqrt(minus1 * minus1 * c->l2_pre + 2.0 * c->lam * minus1 * c->gradient + c->lam * c->lam * c->l2_jnorm);
+  c->eta = std::fabs(std::sqrt(c->l2_new) - lin) / std::sqrt(c->l2_pre);
+  if (eta_safe < 0.1) eta_safe = 0.0;
+  c->eta = std::fmax(c->eta, eta_safe);
+  c->eta = std::fmax(c->eta, eta_min);
+  c->eta = std::fmin(c->eta, eta_max);
+}
+
+static int copy_d2d(msg_ctx *c, double *dst, const double *src, int n) {
+  MSG_CUDA(cudaMemcpyAsync(dst, src, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+  return MSG_OK;
+}
+
+// calc_numsol (Nonlinear_solution.f90:33-294)
+static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
+  const int n = c->N;
+  int rc, maxnun = 0, status = MSG_NEWTON_MAXIT, nan = 0;
+  double maxunk, check_val;
+  msg_stats_t st;
+  memset(&st, 0, sizeof(st));
+  double l2x;
+  if ((rc = dot(c, c->head_new, c->head_new, n, &l2x))) return rc;      // set_backtr
+  c->maxstep = std::sqrt(l2x) * VARMAX;
+  if (c->maxstep < 1.0) c->maxstep = 1.0;
+  for (c->out_iter = 1; c->out_iter <= c->prm.maxout_iter; ++c->out_iter) {
+    if (c->out_iter > 1) c->l2_pre = c->l2_new;
+    c->back_flag = 0; c->back_iter = 0; c->beta_iter = 0;
+    double l2r;
+    if ((rc = make_matvec(c, &l2r))) return rc;
+    if ((rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
+    if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }
+    if ((rc = copy_d2d(c, c->head_pre, c->head_new, n))) return rc;
+    MSG_CUDA(cudaMemsetAsync(c->head_change, 0, (size_t)n * 8, c->stream));
+    c->conv_flag = 0;
+    c->errtol = c->prm.lin_tol > 0 ? c->prm.lin_tol : c->eta;
+    if ((rc = solve_linalg(c, c->l2_pre, c->head_change, &c->l2_jnorm))) return rc;
+    st.inner_total += c->in_iter; st.in_iter_last = c->in_iter;
+    if ((rc = axpby(c, c->head_new, c->head_pre, 1.0, c->head_change, n))) return rc;
+    if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
+    check_val = std::fabs(c->maxvar) * c->len_scal;
+    maxunk = std::fabs(maxunk) * c->len_scal;
+    double crit = c->prm.criteria_rel ? c->prm.criteria * maxunk : c->prm.criteria;
+    if (c->conv_flag != 0 && maxunk == maxunk) {
+      c->conv_flag = 0;
+      if (check_val <= crit && maxunk < XMAX) c->conv_flag = 1;
+    } else if (maxunk != maxunk) {
+      status = MSG_NAN;
+      break;
+    }
+    if (c->conv_flag != 1) {
+      if ((rc = run_backtr(c))) return rc;
+      if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
+      check_val = std::fabs(c->maxvar) * c->len_scal;
+      maxunk = std::fabs(maxunk) * c->len_scal;
+      crit = c->prm.criteria_rel ? c->prm.criteria * maxunk : c->prm.criteria;
+      if (check_val >= VARMAX || maxunk >= XMAX) c->back_flag = 1;
+      else if (check_val <= crit && maxunk < XMAX) c->conv_flag = 1;
+      if (c->conv_flag != 1 && c->back_flag != 1) set_eater(c);
+    }
+    if ((rc = func_norm(c, c->head_new, c->new_f, &c->l2_new))) return rc;
+    st.back_total += c->back_iter; st.back_iter_last = c->back_iter;
+    double conv_var = c->maxvar * c->len_scal;
+    if (c->conv_flag == 1) {
+      if ((rc = copy_d2d(c, c->surf_head, c->head_new, c->S))) return rc;   // calc_surfw
+      status = MSG_OK;
+      break;
+    } else if (c->back_flag == 1) {
+      status = MSG_LINESEARCH_FAIL; break;
+    } else if (c->out_iter == c->prm.maxout_iter) {
+      status = MSG_NEWTON_MAXIT; break;
+    } else if (std::fabs(conv_var) >= VARMAX || maxunk >= XMAX) {
+      status = MSG_DIVERGED; break;
+    }
+  }
+  if (c->out_iter > c->prm.maxout_iter) c->out_iter = c->prm.maxout_iter;
+  st.status = status; st.out_iter = c->out_iter; st.maxnun = maxnun;
+  st.maxvar = c->maxvar * c->len_scal; st.l2_new = c->l2_new;
+  if (stx) *stx = st;
+  return status;
+}
+
+// apply_heuri (Time_module.f90:1522-1543)
+static void apply_heuri(msg_ctx *c, int out_num) {
+  int incr = (int)(c->prm.maxout_iter * 0.4), decr = (int)(c->prm.maxout_iter * 0.8);
+  if (out_num <= incr) c->delt = c->delt_old1 * 1.2;
+  else if (out_num <= decr) c->delt = c->delt_old1;
+  else c->delt = c->delt_old1 * 0.8;
+}
+
+// update_tstep / calc_nextst loop (Time_module.f90:34-273); current_t is real(SP).
+static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after, msg_run_stats_t *rs) {
+  msg_run_stats_t R;
+  memset(&R, 0, sizeof(R));
+  int conv = c->last_conv, last_out = c->last_out, status = MSG_OK, rc;
+  const int n = c->N, S = c->S;
+  while (R.accepted < nsteps) {
+    if (conv == 1) {
+      if (c->timestep_num == 0) c->delt_old1 = c->delt;
+      c->timestep_num++;
+      c->delt_old2 = c->delt_old1; c->delt_old1 = c->delt;
+      if (c->prm.sim_type == 0) c->delt = c->delt * c->prm.inc_fact;
+      else { apply_heuri(c, last_out); if (c->delt > c->prm.max_step) c->delt = c->prm.max_step; }
+      if ((rc = copy_d2d(c, c->head_old, c->head_new, n))) return rc;
+      if ((rc = copy_d2d(c, c->srat_old, c->srat_new, n))) return rc;
+      if ((rc = copy_d2d(c, c->surf_old, c->surf_head, S))) return rc;
+    } else if (conv == 0) {
+      c->current_t = (double)(float)(c->current_t - (double)(float)c->delt);
+      c->delt = c->delt * 0.5;
+      if ((rc = copy_d2d(c, c->head_new, c->head_old, n))) return rc;
+      if ((rc = copy_d2d(c, c->srat_new, c->srat_old, n))) return rc;
+      if ((rc = copy_d2d(c, c->surf_head, c->surf_old, S))) return rc;
+      R.rejected++;
+    }
+    if (c->current_t < rech_until && c->current_t + c->delt > rech_until) c->delt = rech_until - c->current_t;
+    if (c->current_t + c->delt > c->prm.end_time) c->delt = c->prm.end_time - c->current_t;
+    if (c->delt < DSMAL) { status = MSG_DT_TOO_SMALL; break; }
+    double sc = (c->current_t < rech_until) ? 1.0 : rech_after;
+    k_scale_copy<<<nblk(S), kThreads, 0, c->stream>>>(S, c->calc_rech, c->rech_base, sc);
+    MSG_CHECK_LAUNCH();
+    c->current_t = (double)(float)(c->current_t + (double)(float)c->delt);
+    c->delt_inv = 1.0 / c->delt;
+    msg_stats_t st;
+    rc = calc_numsol(c, &st);
+    if (rc < 0) return rc;
+    R.newton_total += st.out_iter; R.krylov_total += st.inner_total; R.back_total += st.back_total;
+    last_out = st.out_iter;
+    conv = (rc == MSG_OK) ? 1 : 0;
+    c->last_out = last_out;
+    if (conv) { R.accepted++; if (c->current_t >= c->prm.end_time) break; }
+  }
+  c->last_conv = conv;
+  R.status = status; R.current_t = c->current_t; R.delt = c->delt;
+  if (rs) *rs = R;
+  return status;
+}
+
+static void free_ctx(msg_ctx *c);
+
+}  // namespace msg
+
+using namespace msg;
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+const char *msg_gpu_last_error(void) { return get_error(); }
+
+#define ALLOC(ptr, bytes) MSG_CUDA(cudaMalloc((void **)&(ptr), (bytes)))
+#define UPLOAD(dst, src, bytes) MSG_CUDA(cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyHostToDevice, c->stream))
+
+static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
+  const size_t N = (size_t)g->nx * g->ny * g->nz, S = (size_t)g->nx * g->ny;
+  c->nx = g->nx; c->ny = g->ny; c->nz = g->nz; c->N = (int)N; c->S = (int)S; c->nxy = (int)S;
+  c->sea_top = g->sea_top; c->free_drainage = g->free_drainage;
+  c->prm = *p;
+  c->len_scal = p->len_scal;
+  c->newper = MACHI_EPS * (double)(1.0f / (float)p->len_scal);   // Prep_calculation.f90:79
+  c->newper_inv = 1.0 / c->newper;
+  c->delt = p->ini_step; c->delt_inv = 1.0 / p->ini_step;
+  c->last_conv = -1;
+  MSG_CUDA(cudaGetDevice(&c->device));
+  MSG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 8; ++k) MSG_CUDA(cudaEventCreate(&c->ev[k]));
+  // symmetric face areas are required by the face-shared DIA storage
+  for (int iz = 0; iz < g->nz; ++iz)
+    for (int iy = 0; iy < g->ny; ++iy)
+      for (int ix = 0; ix < g->nx; ++ix) {
+        size_t i = ix + (size_t)g->nx * (iy + (size_t)g->ny * iz);
+        if (ix > 0 && g->face_area[2 * N + i] != g->face_area[3 * N + i - 1]) {
+          set_error("face areas are not symmetric at cell %zu (west/east)", i);
+          return MSG_ERR_ARG;
+        }
+        if (iy > 0 && g->face_area[1 * N + i] != g->face_area[4 * N + i - g->nx]) {
+          set_error("face areas are not symmetric at cell %zu (north/south)", i);
+          return MSG_ERR_ARG;
+        }
+        if (iz > 0 && g->face_area[0 * N + i] != g->face_area[5 * N + i - S]) {
+          set_error("face areas are not symmetric at cell %zu (up/down)", i);
+          return MSG_ERR_ARG;
+        }
+      }
+  float **fp[] = {&c->reta, &c->retn, &c->resi, &c->poro, &c->ss, &c->ksz};
+  const float *fs[] = {g->reta, g->retn, g->resi, g->poro, g->ss, g->ksz};
+  for (int k = 0; k < 6; ++k) { ALLOC(*fp[k], N * 4); UPLOAD(*fp[k], fs[k], N * 4); }
+  ALLOC(c->cell_top, N * 8); UPLOAD(c->cell_top, g->cell_top, N * 8);
+  ALLOC(c->cell_vol, N * 8); UPLOAD(c->cell_vol, g->cell_vol, N * 8);
+  ALLOC(c->hy, 3 * N * 8); ALLOC(c->ab, 3 * N * 8);
+  double **sp[] = {&c->surf_top, &c->surf_bott, &c->surf_reli, &c->surf_parm, &c->read_seal};
+  const double *ss_[] = {g->surf_top, g->surf_bott, g->surf_reli, g->surf_parm, g->sea_head};
+  for (int k = 0; k < 5; ++k) {
+    ALLOC(*sp[k], S * 8);
+    if (ss_[k]) UPLOAD(*sp[k], ss_[k], S * 8);
+    else MSG_CUDA(cudaMemsetAsync(*sp[k], 0, S * 8, c->stream));
+  }
+  double **sz[] = {&c->hydf_surf, &c->abyd_surf, &c->calc_rech, &c->rech_base, &c->sea_hydf, &c->sea_abyd,
+                   &c->drain, &c->surf_head, &c->surf_old};
+  for (auto q : sz) { ALLOC(*q, S * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, S * 8, c->stream)); }
+  ALLOC(c->offind, (N + 1) * 4);
+  double **vn[] = {&c->head_new, &c->head_old, &c->head_pre, &c->head_change, &c->srat_new, &c->srat_old,
+                   &c->new_f, &c->kr, &c->kr_per, &c->alp, &c->sto, &c->stod, &c->tmpv, &c->dmat, &c->rhs,
+                   &c->slope_rhs, &c->dilu_d, &c->r, &c->rs, &c->p, &c->v, &c->t, &c->z};
+  for (auto q : vn) { ALLOC(*q, N * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, N * 8, c->stream)); }
+  ALLOC(c->lu, 6 * N * 8);
+  size_t npart = std::max((size_t)kRedBlocks * 8, (size_t)nblk((int)N) + 8);
+  ALLOC(c->part, npart * 8);
+  MSG_CUDA(cudaMallocHost((void **)&c->hpin, npart * 8));
+  int rc = build_connectivity(c, g);
+  if (rc) return rc;
+  if (p->precon_type == 0 || p->ref_quirks) {
+    if ((rc = build_wavefront(c))) return rc;
+  }
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t **out) {
+  if (!grid || !params || !out) { set_error("null argument"); return MSG_ERR_ARG; }
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) { set_error("empty grid"); return MSG_ERR_SIZE; }
+  if ((double)grid->nx * grid->ny * grid->nz > 2.0e9 / 6.0) { set_error("grid too large for int32 CSR"); return MSG_ERR_SIZE; }
+  if (params->len_scal <= 0 || params->ini_step <= 0) { set_error("len_scal and ini_step must be positive"); return MSG_ERR_ARG; }
+  if (params->maxout_iter < 1 || params->maxinn_iter < 1) { set_error("iteration caps must be >= 1"); return MSG_ERR_ARG; }
+  const void *req[] = {grid->reta, grid->retn, grid->resi, grid->poro, grid->ss, grid->ksx, grid->ksy, grid->ksz,
+                       grid->cell_top, grid->cell_vol, grid->dis2face, grid->face_area, grid->surf_top, grid->surf_bott};
+  for (auto q : req) if (!q) { set_error("required grid array is NULL"); return MSG_ERR_ARG; }
+  msg_ctx *c = new (std::nothrow) msg_ctx();
+  if (!c) { set_error("out of host memory"); return MSG_ERR_ARG; }
+  memset(c, 0, sizeof(*c));
+  int rc = create_impl(c, grid, params);
+  if (rc) { free_ctx(c); return rc; }
+  *out = c;
+  return MSG_OK;
+}
+
+void msg_gpu_destroy(msg_ctx_t *c) {
+  if (c) free_ctx(c);
+}
+
+int msg_gpu_get_connect(msg_ctx_t *c, int32_t *offind, int32_t *offrow, int32_t *conn_dir, int32_t *left_off,
+                        int32_t *right_off, double *hydf_conn, double *abyd_conn, int32_t *nnz) {
+  if (!c) return MSG_ERR_ARG;
+  size_t M = c->nnz;
+  if (offind) MSG_CUDA(cudaMemcpy(offind, c->offind, (c->N + 1) * 4, cudaMemcpyDeviceToHost));
+  if (offrow) MSG_CUDA(cudaMemcpy(offrow, c->offrow, M * 4, cudaMemcpyDeviceToHost));
+  if (conn_dir) MSG_CUDA(cudaMemcpy(conn_dir, c->conn_dir, M * 4, cudaMemcpyDeviceToHost));
+  if (left_off) MSG_CUDA(cudaMemcpy(left_off, c->left_off, M * 4, cudaMemcpyDeviceToHost));
+  if (right_off) MSG_CUDA(cudaMemcpy(right_off, c->right_off, M * 4, cudaMemcpyDeviceToHost));
+  if (hydf_conn) MSG_CUDA(cudaMemcpy(hydf_conn, c->hydf_conn, M * 8, cudaMemcpyDeviceToHost));
+  if (abyd_conn) MSG_CUDA(cudaMemcpy(abyd_conn, c->abyd_conn, M * 8, cudaMemcpyDeviceToHost));
+  if (nnz) *nnz = c->nnz;
+  return MSG_OK;
+}
+
+int msg_gpu_init_state(msg_ctx_t *c, const double *head, double delt) {
+  if (!c || !head || delt <= 0) return MSG_ERR_ARG;
+  size_t N = c->N, S = c->S;
+  UPLOAD(c->head_new, head, N * 8);
+  MSG_CUDA(cudaMemcpyAsync(c->head_old, c->head_new, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  int rc = launch_srat_rperm(c, c->head_new, 0.0, c->srat_old, c->kr, nullptr);
+  if (rc) return rc;
+  MSG_CUDA(cudaMemcpyAsync(c->srat_new, c->srat_old, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  MSG_CUDA(cudaMemcpyAsync(c->surf_head, c->head_new, S * 8, cudaMemcpyDeviceToDevice, c->stream));
+  MSG_CUDA(cudaMemcpyAsync(c->surf_old, c->head_new, S * 8, cudaMemcpyDeviceToDevice, c->stream));
+  c->delt = delt; c->delt_inv = 1.0 / delt;
+  c->current_t = 0.0; c->timestep_num = 0; c->delt_old1 = 0.0; c->last_conv = -1; c->last_out = 0;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_set_state(msg_ctx_t *c, const double *head_new, const double *head_old, const double *srat_old,
+                      const double *surf_head, double delt) {
+  if (!c) return MSG_ERR_ARG;
+  size_t N = c->N, S = c->S;
+  if (head_new) UPLOAD(c->head_new, head_new, N * 8);
+  if (head_old) UPLOAD(c->head_old, head_old, N * 8);
+  if (srat_old) UPLOAD(c->srat_old, srat_old, N * 8);
+  if (surf_head) { UPLOAD(c->surf_head, surf_head, S * 8); UPLOAD(c->surf_old, surf_head, S * 8); }
+  if (delt > 0) { c->delt = delt; c->delt_inv = 1.0 / delt; }
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_get_state(msg_ctx_t *c, double *head_new, double *head_old, double *srat_new, double *srat_old,
+                      double *surf_head) {
+  if (!c) return MSG_ERR_ARG;
+  size_t N = c->N, S = c->S;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  if (head_new) MSG_CUDA(cudaMemcpy(head_new, c->head_new, N * 8, cudaMemcpyDeviceToHost));
+  if (head_old) MSG_CUDA(cudaMemcpy(head_old, c->head_old, N * 8, cudaMemcpyDeviceToHost));
+  if (srat_new) MSG_CUDA(cudaMemcpy(srat_new, c->srat_new, N * 8, cudaMemcpyDeviceToHost));
+  if (srat_old) MSG_CUDA(cudaMemcpy(srat_old, c->srat_old, N * 8, cudaMemcpyDeviceToHost));
+  if (surf_head) MSG_CUDA(cudaMemcpy(surf_head, c->surf_head, S * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_set_recharge(msg_ctx_t *c, const double *calc_rech) {
+  if (!c || !calc_rech) return MSG_ERR_ARG;
+  UPLOAD(c->rech_base, calc_rech, (size_t)c->S * 8);
+  UPLOAD(c->calc_rech, calc_rech, (size_t)c->S * 8);
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_srat_rperm(msg_ctx_t *c, const double *pres, double pertur, double *srat, double *rperm, double *sstor) {
+  if (!c || !pres) return MSG_ERR_ARG;
+  size_t N = c->N;
+  UPLOAD(c->tmpv, pres, N * 8);
+  int rc = launch_srat_rperm(c, c->tmpv, pertur, c->v, c->t, c->z);
+  if (rc) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  if (srat) MSG_CUDA(cudaMemcpy(srat, c->v, N * 8, cudaMemcpyDeviceToHost));
+  if (rperm) MSG_CUDA(cudaMemcpy(rperm, c->t, N * 8, cudaMemcpyDeviceToHost));
+  if (sstor) MSG_CUDA(cudaMemcpy(sstor, c->z, N * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_calc_func(msg_ctx_t *c, const double *infx, double *funcv) {
+  if (!c || !infx || !funcv) return MSG_ERR_ARG;
+  size_t N = c->N;
+  UPLOAD(c->tmpv, infx, N * 8);
+  int rc = launch_calc_func(c, c->tmpv, c->new_f, false);
+  if (rc) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  MSG_CUDA(cudaMemcpy(funcv, c->new_f, N * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_make_matvec(msg_ctx_t *c, double *dmat, double *lumat, double *rhs) {
+  if (!c) return MSG_ERR_ARG;
+  double l2;
+  int rc = make_matvec(c, &l2);
+  if (rc) return rc;
+  size_t N = c->N;
+  if (lumat) {
+    double *tmp = nullptr;
+    ALLOC(tmp, (size_t)c->nnz * 8);
+    if ((rc = launch_dia_to_csr(c, tmp))) return rc;
+    MSG_CUDA(cudaStreamSynchronize(c->stream));
+    MSG_CUDA(cudaMemcpy(lumat, tmp, (size_t)c->nnz * 8, cudaMemcpyDeviceToHost));
+    cudaFree(tmp);
+  }
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  if (dmat) MSG_CUDA(cudaMemcpy(dmat, c->dmat, N * 8, cudaMemcpyDeviceToHost));
+  if (rhs) MSG_CUDA(cudaMemcpy(rhs, c->rhs, N * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_set_system(msg_ctx_t *c, const double *dmat, const double *lumat, const double *rhs) {
+  if (!c || !dmat || !lumat || !rhs) return MSG_ERR_ARG;
+  size_t N = c->N;
+  UPLOAD(c->dmat, dmat, N * 8);
+  UPLOAD(c->rhs, rhs, N * 8);
+  double *tmp = nullptr;
+  ALLOC(tmp, (size_t)c->nnz * 8);
+  UPLOAD(tmp, lumat, (size_t)c->nnz * 8);
+  k_csr_to_dia<<<nblk(c->N), kThreads, 0, c->stream>>>(c->nx, c->ny, c->nz, c->offind, tmp, c->lu);
+  MSG_CHECK_LAUNCH();
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(tmp);
+  MSG_CUDA(cudaMemcpyAsync(c->slope_rhs, c->rhs, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->prm.precon_type == 1 && !c->prm.ref_quirks) {
+    int rc = amg_setup(c);
+    if (rc) return rc;
+  }
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_precond(msg_ctx_t *c, const double *r, double *z) {
+  if (!c || !r || !z) return MSG_ERR_ARG;
+  size_t N = c->N;
+  int rc;
+  if (c->prm.precon_type == 0 || c->prm.ref_quirks) {
+    if ((rc = launch_precon_dilu(c))) return rc;
+  }
+  UPLOAD(c->tmpv, r, N * 8);
+  if ((rc = apply_prec(c, c->tmpv, c->z))) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  MSG_CUDA(cudaMemcpy(z, c->z, N * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_solve_linalg(msg_ctx_t *c, double init_norm, double errtol, double *inx, double *last_norm,
+                         int32_t *in_iter, int32_t *conv_flag) {
+  if (!c || !inx) return MSG_ERR_ARG;
+  size_t N = c->N;
+  UPLOAD(c->head_change, inx, N * 8);
+  c->errtol = errtol;
+  double ln = 0.0;
+  int rc = solve_linalg(c, init_norm, c->head_change, &ln);
+  if (rc) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  MSG_CUDA(cudaMemcpy(inx, c->head_change, N * 8, cudaMemcpyDeviceToHost));
+  if (last_norm) *last_norm = ln;
+  if (in_iter) *in_iter = c->in_iter;
+  if (conv_flag) *conv_flag = c->conv_flag;
+  return MSG_OK;
+}
+
+int msg_gpu_vecjacf(msg_ctx_t *c, const double *x, const double *v, double *out) {
+  if (!c || !x || !v || !out) return MSG_ERR_ARG;
+  size_t N = c->N;
+  UPLOAD(c->head_pre, x, N * 8);
+  UPLOAD(c->head_change, v, N * 8);
+  int rc = vecjacf(c, c->head_pre, c->head_change, c->tmpv);
+  if (rc) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  MSG_CUDA(cudaMemcpy(out, c->tmpv, N * 8, cudaMemcpyDeviceToHost));
+  return MSG_OK;
+}
+
+int msg_gpu_calc_numsol(msg_ctx_t *c, msg_stats_t *stats) {
+  if (!c) return MSG_ERR_ARG;
+  memset(c->t_ms, 0, sizeof(c->t_ms));
+  return calc_numsol(c, stats);
+}
+
+int msg_gpu_advance(msg_ctx_t *c, int32_t nsteps, double rech_until, double rech_after, msg_run_stats_t *stats) {
+  if (!c || nsteps < 0) return MSG_ERR_ARG;
+  memset(c->t_ms, 0, sizeof(c->t_ms));
+  cudaEventRecord(c->ev[5], c->stream);
+  int rc = advance(c, nsteps, rech_until, rech_after, stats);
+  cudaEventRecord(c->ev[6], c->stream);
+  cudaEventSynchronize(c->ev[6]);
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, c->ev[5], c->ev[6]);
+  c->t_ms[4] = tot;
+  return rc;
+}
+
+int msg_gpu_calc_mass(msg_ctx_t *c, double *out9) {
+  if (!c || !out9) return MSG_ERR_ARG;
+  double *d = nullptr;
+  ALLOC(d, 9 * 8);
+  int rc = launch_mass(c, d);
+  if (rc) return rc;
+  MSG_CUDA(cudaMemcpy(out9, d, 9 * 8, cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return MSG_OK;
+}
+
+int msg_gpu_timers(msg_ctx_t *c, double *ms5) {
+  if (!c || !ms5) return MSG_ERR_ARG;
+  for (int k = 0; k < 5; ++k) ms5[k] = c->t_ms[k];
+  return MSG_OK;
+}
+
+long long msg_gpu_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+// Time `reps` back-to-back launches of one kernel class on the context's stream
+// with CUDA events (the state of the last step is used as input):
+// 0 = stencil SpMV (FP64 DIA), 1 = calc_func (vG pass + flux pass),
+// 2 = make_matvec (vG pair + assembly), 3 = preconditioner apply, 4 = AMG setup.
+int msg_gpu_kernel_time(msg_ctx_t *c, int32_t which, int32_t reps, double *ms_per_launch) {
+  if (!c || reps < 1 || !ms_per_launch) return MSG_ERR_ARG;
+  int rc = MSG_OK;
+  if (which == 3 && (c->prm.precon_type == 0 || c->prm.ref_quirks)) {
+    if ((rc = launch_precon_dilu(c))) return rc;
+  }
+  auto one = [&]() -> int {
+    switch (which) {
+      case 0: return launch_spmv(c, c->head_new, c->tmpv);
+      case 1: return launch_calc_func(c, c->head_new, c->new_f, false);
+      case 2: return launch_make_matvec(c);
+      case 3: return apply_prec(c, c->rhs, c->z);
+      case 4: return (c->prm.precon_type == 1 && !c->prm.ref_quirks) ? amg_setup(c) : MSG_OK;
+      default: return MSG_ERR_ARG;
+    }
+  };
+  if ((rc = one())) return rc;   // warm-up
+  MSG_CUDA(cudaEventRecord(c->ev[5], c->stream));
+  for (int k = 0; k < reps; ++k)
+    if ((rc = one())) return rc;
+  MSG_CUDA(cudaEventRecord(c->ev[6], c->stream));
+  MSG_CUDA(cudaEventSynchronize(c->ev[6]));
+  float ms = 0.f;
+  MSG_CUDA(cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]));
+  *ms_per_launch = (double)ms / reps;
+  return MSG_OK;
+}
+
+int msg_gpu_set_timing(msg_ctx_t *c, int32_t on) {
+  if (!c) return MSG_ERR_ARG;
+  c->timing = on;
+  return MSG_OK;
+}
+
+}  // extern "C"
+
+namespace msg {
+static void free_ctx(msg_ctx *c) {
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  amg_free(c);
+  void *dp[] = {c->reta, c->retn, c->resi, c->poro, c->ss, c->ksz, c->cell_top, c->cell_vol, c->hy, c->ab,
+                c->surf_top, c->surf_bott, c->surf_reli, c->surf_parm, c->hydf_surf, c->abyd_surf, c->calc_rech,
+                c->rech_base, c->sea_hydf, c->sea_abyd, c->read_seal, c->drain, c->offind, c->offrow, c->conn_dir,
+                c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,
+                c->head_change, c->srat_new, c->srat_old, c->surf_head, c->surf_old, c->new_f, c->kr, c->kr_per,
+                c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->slope_rhs, c->dilu_d, c->r, c->rs,
+                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells};
+  for (auto q : dp) if (q) cudaFree(q);
+  if (c->hpin) cudaFreeHost(c->hpin);
+  for (int k = 0; k < 8; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+}  // namespace msg

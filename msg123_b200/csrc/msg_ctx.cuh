@@ -1,0 +1,111 @@
+// msg_ctx.cuh -- device-side state of one solver context and the internal host API
+// between the translation units of libmsg123gpu.so.
+#pragma once
+#include "msg_common.cuh"
+#include "../../include/msg123_gpu.h"
+
+namespace msg {
+
+struct AmgLevel;   // msg_amg.cu
+
+// Scalars of the Krylov / Newton recurrences kept in device memory.
+struct DevScalars {
+  double sk, sk0, sk2, alpha, beta, omega, ts, tt, rnorm, bnorm, errtol;
+  int conv, in_iter, done, pad;
+};
+
+}  // namespace msg
+
+struct msg_ctx {
+  // ---- sizes --------------------------------------------------------------------
+  int nx, ny, nz, N, S, nxy, nnz;
+  int sea_top, free_drainage;
+  msg_params_t prm;
+  double len_scal, newper, newper_inv;
+  double delt, delt_inv;
+  int device;
+  cudaStream_t stream;
+
+  // ---- cell data (structured, reference local order) ------------------------------
+  float *reta, *retn, *resi, *poro, *ss;        // [N] real(SP)
+  double *cell_top, *cell_vol;                   // [N]
+  double *hy, *ab;                               // [3N] hydf / abyd of the up, north, west face of each cell
+  float *ksz;                                    // [N] kept for the drainage and surface coefficients
+  // ---- surface (top layer) and boundary arrays [S] -----------------------------------
+  double *surf_top, *surf_bott, *surf_reli, *surf_parm, *hydf_surf, *abyd_surf;
+  double *calc_rech, *rech_base;
+  double *sea_hydf, *sea_abyd, *read_seal;
+  double *drain;                                 // [S] bottom-layer drainage coefficient
+  // ---- reference CSR built on the GPU (export / tests) -------------------------------
+  int *offind, *offrow, *conn_dir, *left_off, *right_off;
+  double *hydf_conn, *abyd_conn;
+  // ---- state -------------------------------------------------------------------------
+  double *head_new, *head_old, *head_pre, *head_change, *srat_new, *srat_old;
+  double *surf_head, *surf_old, *new_f;
+  double *kr, *kr_per, *alp, *sto, *stod;        // per-cell vG results / storage terms
+  double *tmpv;                                  // [N] spare vector (J.v, line search)
+  // ---- level-1 system, DIA: lu[d*N + i] = J(i, nb_d(i)) --------------------------------
+  double *dmat, *lu, *rhs, *slope_rhs;
+  // ---- Krylov work ----------------------------------------------------------------------
+  double *dilu_d, *r, *rs, *p, *v, *t, *z;
+  msg::DevScalars *sc;                           // device scalars
+  msg::DevScalars *sc_host;                      // pinned mirror
+  double *part;                                  // reduction partials [kRedBlocks * 8]
+  double *hpin;                                  // pinned host scalars [64]
+  // ---- wavefront ordering for DILU --------------------------------------------------------
+  int *plane_ptr, *plane_cells;
+  int nplanes;
+  // ---- AMG ----------------------------------------------------------------------------------
+  msg::AmgLevel *amg;
+  int amg_nlevel;
+  // ---- Newton module variables (Nonlinear_solution.f90:24-27) ---------------------------------
+  int back_iter, back_flag, beta_iter, in_iter, conv_flag, out_iter;
+  double maxvar, l2_new, l2_pre, l2_jnorm, lam, eta, gradient, maxstep, errtol, bnorm, rnorm;
+  // ---- time loop ---------------------------------------------------------------------------------
+  double current_t, delt_old1, delt_old2;
+  int timestep_num, last_conv, last_out;
+  // ---- timing ------------------------------------------------------------------------------------
+  cudaEvent_t ev[8];
+  double t_ms[5];
+  int timing;
+};
+
+namespace msg {
+
+// ---- msg_physics.cu ---------------------------------------------------------------------------
+int build_connectivity(msg_ctx *c, const msg_grid_t *g);
+int launch_srat_rperm(msg_ctx *c, const double *h, double pertur, double *srat, double *kr, double *alp);
+// F = calc_func(h); also writes srat_new and kr (rel_perm).  partial sums of F^2 in c->part[0..].
+int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm);
+// make_matvec at c->head_new: dmat, lu (DIA), rhs = -F.
+int launch_make_matvec(msg_ctx *c);
+// Export the DIA Jacobian into the reference CSR order.
+int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
+int launch_mass(msg_ctx *c, double *out9_dev);
+
+// ---- msg_linear.cu ----------------------------------------------------------------------------
+int build_wavefront(msg_ctx *c);
+int launch_precon_dilu(msg_ctx *c);
+int launch_solve_ilu(msg_ctx *c, const double *b, double *x);
+int launch_spmv(msg_ctx *c, const double *x, double *y);
+int solve_bicgs(msg_ctx *c, double *x);      // x in/out (device), uses c->rhs, c->bnorm, c->errtol
+// reductions (results land in c->hpin after a sync)
+int dot(msg_ctx *c, const double *a, const double *b, int n, double *out);   // sync + host value
+int norm1(msg_ctx *c, const double *a, int n, double *out);
+int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan);
+int lam_length(msg_ctx *c, const double *dh, const double *hn, double *out);
+int axpby(msg_ctx *c, double *y, const double *x, double a, const double *w, int n);   // y = x + a*w
+int scale(msg_ctx *c, double *y, double a, int n);
+
+// ---- msg_amg.cu ---------------------------------------------------------------------------------
+int amg_setup(msg_ctx *c);
+int amg_apply(msg_ctx *c, const double *r, double *z);
+void amg_free(msg_ctx *c);
+
+// ---- preconditioner dispatch (msg_linear.cu) ---------------------------------------------------------
+int apply_prec(msg_ctx *c, const double *r, double *z);
+
+// ---- scan (msg_linear.cu) ---------------------------------------------------------------------------
+int scan_exclusive(msg_ctx *c, const int *in, int *out, int n, int *total_host);
+
+}  // namespace msg

@@ -1,0 +1,229 @@
+"""Host-side mirror of Msg123's solver interface over libmsg123gpu.so.
+
+``GpuSolver`` exposes the reference routines under their reference names:
+
+* ``calc_func(h)``            -- Calc_function.f90:24-101
+* ``srat_rperm(h, pertur)``   -- Calc_parameter.f90:15-77
+* ``make_matvec()``           -- Make_linearsystem.f90:24-68
+* ``solve_linalg(...)``       -- Linear_solution.f90:26-58
+* ``calc_numsol()``           -- Nonlinear_solution.f90:33-294
+* ``advance(nsteps)``         -- Msg.f90:83-104 with Time_module.f90:34-273
+* ``calc_mass()``             -- Calc_function.f90:103-174
+
+Every call goes through the C ABI declared in include/msg123_gpu.h.  There is no
+CPU fallback: if the CUDA library is missing or no GPU is present the
+constructor raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import dptr, iptr
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmsg123gpu.so")
+_lib = None
+
+
+class MsgError(RuntimeError):
+    pass
+
+
+def load_library():
+    """Load libmsg123gpu.so (built in-tree by msg123_b200/build.py) or raise."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MsgError(f"{LIB_PATH} is missing: run `python -m msg123_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.msg_gpu_last_error.restype = C.c_char_p
+    L.msg_gpu_create.argtypes = [C.POINTER(abi.MsgGrid), C.POINTER(abi.MsgParams), C.POINTER(vp)]
+    L.msg_gpu_destroy.argtypes = [vp]
+    L.msg_gpu_destroy.restype = None
+    L.msg_gpu_get_connect.argtypes = [vp, abi.PI, abi.PI, abi.PI, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI]
+    L.msg_gpu_init_state.argtypes = [vp, abi.PD, C.c_double]
+    L.msg_gpu_set_state.argtypes = [vp, abi.PD, abi.PD, abi.PD, abi.PD, C.c_double]
+    L.msg_gpu_get_state.argtypes = [vp, abi.PD, abi.PD, abi.PD, abi.PD, abi.PD]
+    L.msg_gpu_set_recharge.argtypes = [vp, abi.PD]
+    L.msg_gpu_srat_rperm.argtypes = [vp, abi.PD, C.c_double, abi.PD, abi.PD, abi.PD]
+    L.msg_gpu_calc_func.argtypes = [vp, abi.PD, abi.PD]
+    L.msg_gpu_make_matvec.argtypes = [vp, abi.PD, abi.PD, abi.PD]
+    L.msg_gpu_set_system.argtypes = [vp, abi.PD, abi.PD, abi.PD]
+    L.msg_gpu_precond.argtypes = [vp, abi.PD, abi.PD]
+    L.msg_gpu_vecjacf.argtypes = [vp, abi.PD, abi.PD, abi.PD]
+    L.msg_gpu_solve_linalg.argtypes = [vp, C.c_double, C.c_double, abi.PD, abi.PD, abi.PI, abi.PI]
+    L.msg_gpu_calc_numsol.argtypes = [vp, C.POINTER(abi.MsgStats)]
+    L.msg_gpu_advance.argtypes = [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.MsgRunStats)]
+    L.msg_gpu_calc_mass.argtypes = [vp, abi.PD]
+    L.msg_gpu_timers.argtypes = [vp, abi.PD]
+    L.msg_gpu_set_timing.argtypes = [vp, C.c_int32]
+    L.msg_gpu_kernel_time.argtypes = [vp, C.c_int32, C.c_int32, abi.PD]
+    L.msg_gpu_launch_count.restype = C.c_longlong
+    L.msg_gpu_launch_count.argtypes = []
+    _lib = L
+    return L
+
+
+def launch_count():
+    return int(load_library().msg_gpu_launch_count())
+
+
+def _check(rc, what):
+    if rc < 0:
+        msg = load_library().msg_gpu_last_error().decode(errors="replace")
+        raise MsgError(f"{what} failed ({abi.STATUS_NAMES.get(rc, rc)}): {msg}")
+    return rc
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class GpuSolver:
+    """One solver context on the current CUDA device for a config.Problem."""
+
+    def __init__(self, prob, **overrides):
+        L = load_library()
+        self.prob = prob
+        prm = dict(prob.params)
+        prm.update(overrides)
+        self.params = prm
+        self._g = abi.fill_grid(prob)
+        self._p = abi.fill_params(prm)
+        h = C.c_void_p()
+        _check(L.msg_gpu_create(C.byref(self._g), C.byref(self._p), C.byref(h)), "msg_gpu_create")
+        self.h = h
+        self.n = prob.ncalc
+        self.ncals = prob.ncals
+        nnz = C.c_int32()
+        _check(L.msg_gpu_get_connect(self.h, None, None, None, None, None, None, None, C.byref(nnz)), "get_connect")
+        self.nnz = nnz.value
+        self.set_recharge(prob.rech)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().msg_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- topology ---------------------------------------------------------------------
+    def connect(self):
+        N, M = self.n, self.nnz
+        out = dict(offind=np.zeros(N + 1, np.int32), offrow=np.zeros(M, np.int32), conn_dir=np.zeros(M, np.int32),
+                   left_off=np.zeros(M, np.int32), right_off=np.zeros(M, np.int32),
+                   hydf=np.zeros(M), abyd=np.zeros(M))
+        _check(load_library().msg_gpu_get_connect(self.h, iptr(out["offind"]), iptr(out["offrow"]),
+                                                  iptr(out["conn_dir"]), iptr(out["left_off"]),
+                                                  iptr(out["right_off"]), dptr(out["hydf"]), dptr(out["abyd"]),
+                                                  None), "get_connect")
+        return out
+
+    # -- state --------------------------------------------------------------------------
+    def init_state(self, head=None, delt=None):
+        head = self.prob.head0 if head is None else head
+        delt = self.params["ini_step"] if delt is None else delt
+        _check(load_library().msg_gpu_init_state(self.h, dptr(_f64(head)), C.c_double(delt)), "init_state")
+
+    def set_state(self, head_new=None, head_old=None, srat_old=None, surf_head=None, delt=0.0):
+        arrs = [None if a is None else _f64(a) for a in (head_new, head_old, srat_old, surf_head)]
+        _check(load_library().msg_gpu_set_state(self.h, *(dptr(a) for a in arrs), C.c_double(delt)), "set_state")
+
+    def get_state(self):
+        N, S = self.n, self.ncals
+        out = dict(head_new=np.zeros(N), head_old=np.zeros(N), srat_new=np.zeros(N), srat_old=np.zeros(N),
+                   surf_head=np.zeros(S))
+        _check(load_library().msg_gpu_get_state(self.h, *(dptr(out[k]) for k in
+                                                         ("head_new", "head_old", "srat_new", "srat_old",
+                                                          "surf_head"))), "get_state")
+        return out
+
+    def set_recharge(self, rech):
+        _check(load_library().msg_gpu_set_recharge(self.h, dptr(_f64(rech))), "set_recharge")
+
+    # -- reference routines -----------------------------------------------------------------
+    def srat_rperm(self, pres, pertur=0.0):
+        N = self.n
+        s, k, ss = np.zeros(N), np.zeros(N), np.zeros(N)
+        _check(load_library().msg_gpu_srat_rperm(self.h, dptr(_f64(pres)), C.c_double(pertur), dptr(s), dptr(k),
+                                                 dptr(ss)), "srat_rperm")
+        return s, k, ss
+
+    def calc_func(self, x):
+        f = np.zeros(self.n)
+        _check(load_library().msg_gpu_calc_func(self.h, dptr(_f64(x)), dptr(f)), "calc_func")
+        return f
+
+    def make_matvec(self):
+        d, lu, r = np.zeros(self.n), np.zeros(self.nnz), np.zeros(self.n)
+        _check(load_library().msg_gpu_make_matvec(self.h, dptr(d), dptr(lu), dptr(r)), "make_matvec")
+        return d, lu, r
+
+    def set_system(self, dmat, lumat, rhs):
+        _check(load_library().msg_gpu_set_system(self.h, dptr(_f64(dmat)), dptr(_f64(lumat)), dptr(_f64(rhs))),
+               "set_system")
+
+    def precond(self, r):
+        z = np.zeros(self.n)
+        _check(load_library().msg_gpu_precond(self.h, dptr(_f64(r)), dptr(z)), "precond")
+        return z
+
+    def vecjacf(self, x, v):
+        out = np.zeros(self.n)
+        _check(load_library().msg_gpu_vecjacf(self.h, dptr(_f64(x)), dptr(_f64(v)), dptr(out)), "vecjacf")
+        return out
+
+    def solve_linalg(self, init_norm, errtol, x0=None):
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        last = C.c_double()
+        it = C.c_int32()
+        conv = C.c_int32()
+        _check(load_library().msg_gpu_solve_linalg(self.h, C.c_double(init_norm), C.c_double(errtol), dptr(x),
+                                                   C.byref(last), C.byref(it), C.byref(conv)), "solve_linalg")
+        return x, last.value, it.value, conv.value
+
+    def calc_numsol(self):
+        st = abi.MsgStats()
+        rc = _check(load_library().msg_gpu_calc_numsol(self.h, C.byref(st)), "calc_numsol")
+        return rc, st.as_dict()
+
+    def advance(self, nsteps=None, rech_until=None, rech_after=None):
+        nsteps = self.prob.nsteps if nsteps is None else nsteps
+        ru = self.prob.rech_until if rech_until is None else rech_until
+        ra = self.prob.rech_after if rech_after is None else rech_after
+        rs = abi.MsgRunStats()
+        rc = _check(load_library().msg_gpu_advance(self.h, int(nsteps), C.c_double(ru), C.c_double(ra), C.byref(rs)),
+                    "advance")
+        return rc, rs.as_dict()
+
+    def calc_mass(self):
+        out = np.zeros(9)
+        _check(load_library().msg_gpu_calc_mass(self.h, dptr(out)), "calc_mass")
+        return out
+
+    def set_timing(self, on=True):
+        _check(load_library().msg_gpu_set_timing(self.h, int(bool(on))), "set_timing")
+
+    def kernel_time(self, which, reps=20):
+        ms = C.c_double()
+        _check(load_library().msg_gpu_kernel_time(self.h, int(which), int(reps), C.byref(ms)), "kernel_time")
+        return ms.value
+
+    def timers(self):
+        out = np.zeros(5)
+        _check(load_library().msg_gpu_timers(self.h, dptr(out)), "timers")
+        return dict(zip(("assembly_ms", "krylov_ms", "amg_setup_ms", "residual_ms", "total_ms"), out.tolist()))
