@@ -196,6 +196,16 @@ MSG_API int msg_gpu_timers(msg_ctx_t *ctx, double *ms5);
  * 2 = make_matvec, 3 = one preconditioner apply, 4 = AMG setup.  Result in ms per launch. */
 MSG_API int msg_gpu_kernel_time(msg_ctx_t *ctx, int32_t which, int32_t reps, double *ms_per_launch);
 
+/* AMG hierarchy of the last setup (structural tests): level 0 is the Jacobian in CSR
+ * form; level l > 0 holds its operator (off-diagonals CSR, 0-based columns, diagonal
+ * apart as in array_var(l)%{dmat,lumat}), the prolongation P from it to level l-1 and
+ * the aggregate of every level l-1 row (-1: none).  No counterpart returns these in
+ * the reference; they mirror pro_var / crs_index / array_var (Allocate_solution.f90:22-50). */
+MSG_API int msg_gpu_amg_nlevel(msg_ctx_t *ctx);
+MSG_API int msg_gpu_amg_level_sizes(msg_ctx_t *ctx, int32_t lv, int32_t *n, int32_t *nnz, int32_t *pnnz);
+MSG_API int msg_gpu_amg_level(msg_ctx_t *ctx, int32_t lv, int32_t *offind, int32_t *offrow, double *dmat,
+                              double *lumat, int32_t *pindex, int32_t *poffrow, double *pval, int32_t *agg);
+
 /* Number of kernels this library has launched in this process (all contexts). */
 MSG_API long long msg_gpu_launch_count(void);
 

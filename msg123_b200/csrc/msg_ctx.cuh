@@ -56,7 +56,7 @@ struct msg_ctx {
   int *plane_ptr, *plane_cells;
   int nplanes;
   // ---- AMG ----------------------------------------------------------------------------------
-  msg::AmgLevel *amg;
+  void *amg;                                     // msg::AmgState (msg_amg.cu)
   int amg_nlevel;
   // ---- Newton module variables (Nonlinear_solution.f90:24-27) ---------------------------------
   int back_iter, back_flag, beta_iter, in_iter, conv_flag, out_iter;

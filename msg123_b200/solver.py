@@ -62,6 +62,9 @@ def load_library():
     L.msg_gpu_timers.argtypes = [vp, abi.PD]
     L.msg_gpu_set_timing.argtypes = [vp, C.c_int32]
     L.msg_gpu_kernel_time.argtypes = [vp, C.c_int32, C.c_int32, abi.PD]
+    L.msg_gpu_amg_nlevel.argtypes = [vp]
+    L.msg_gpu_amg_level_sizes.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PI]
+    L.msg_gpu_amg_level.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
     L.msg_gpu_launch_count.restype = C.c_longlong
     L.msg_gpu_launch_count.argtypes = []
     _lib = L
@@ -214,6 +217,27 @@ class GpuSolver:
         out = np.zeros(9)
         _check(load_library().msg_gpu_calc_mass(self.h, dptr(out)), "calc_mass")
         return out
+
+    def amg_levels(self):
+        """The AMG hierarchy of the last setup (level 0 = Jacobian), as numpy arrays."""
+        L = load_library()
+        levels = []
+        for lv in range(L.msg_gpu_amg_nlevel(self.h)):
+            n, nnz, pnnz = C.c_int32(), C.c_int32(), C.c_int32()
+            _check(L.msg_gpu_amg_level_sizes(self.h, lv, C.byref(n), C.byref(nnz), C.byref(pnnz)), "amg sizes")
+            n, nnz, pnnz = n.value, nnz.value, pnnz.value
+            d = dict(n=n, offind=np.zeros(n + 1, np.int32), offrow=np.zeros(max(nnz, 1), np.int32)[:nnz],
+                     dmat=np.zeros(n), lumat=np.zeros(max(nnz, 1))[:nnz])
+            args = [None, None, None, None]
+            if lv > 0:
+                nf = levels[-1]["n"]
+                d.update(pindex=np.zeros(nf + 1, np.int32), poffrow=np.zeros(max(pnnz, 1), np.int32)[:pnnz],
+                         pval=np.zeros(max(pnnz, 1))[:pnnz], agg=np.zeros(nf, np.int32))
+                args = [iptr(d["pindex"]), iptr(d["poffrow"]), dptr(d["pval"]), iptr(d["agg"])]
+            _check(L.msg_gpu_amg_level(self.h, lv, iptr(d["offind"]), iptr(d["offrow"]), dptr(d["dmat"]),
+                                       dptr(d["lumat"]), *args), "amg level")
+            levels.append(d)
+        return levels
 
     def set_timing(self, on=True):
         _check(load_library().msg_gpu_set_timing(self.h, int(bool(on))), "set_timing")

@@ -593,6 +593,8 @@ static void solve_linalg(orc_t *o, double init_norm, double *inx, double *last_n
  *               ascending column order; same accumulation rule; diagonal split off.
  * =================================================================================*/
 #define MIS_UNDEC 1ull
+#define P_ROW_MAX 96      /* longest prolongation row before coarsening stops */
+#define HASH_MAX 700      /* most distinct columns of a product row before coarsening stops */
 #define MIS_ROOT 2ull
 
 static inline uint32_t mis_hash(uint32_t x, uint32_t lev) {
@@ -703,7 +705,7 @@ static int own_coarsen(orc_t *o, int lv) {
     for (int i = 0; i < n; ++i) {
       if (st[i] != MIS_UNDEC) continue;
       if ((uint32_t)(t2[i] & 0xffffffffu) == (uint32_t)i) st[i] = MIS_ROOT;
-      else if ((t2[i] >> 62) == MIS_ROOT) st[i] = 3;   /* non-root (decided) */
+      else if ((t2[i] >> 62) == MIS_ROOT) st[i] = 0;   /* decided non-root: drops out of the max */
     }
   }
   /* aggregate numbering: roots in index order */
@@ -735,6 +737,20 @@ static int own_coarsen(orc_t *o, int lv) {
   free(agg2); free(st); free(t0); free(t1); free(t2);
   free(g_last_agg[lv]); g_last_agg[lv] = agg;
   if (nc == 0 || nc >= n) { free(sidx); free(slu); free(tdm); return 0; }
+  /* rows of P longer than P_ROW_MAX stop the coarsening (the GPU keeps them in registers) */
+  for (int i = 0; i < n; ++i) {
+    int cnt = 0, lst[P_ROW_MAX + 1];
+    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+      int J = agg[F->offrow[slu[s]]], q;
+      if (J < 0) continue;
+      for (q = 0; q < cnt; ++q) if (lst[q] == J) break;
+      if (q == cnt) { if (cnt == P_ROW_MAX) { free(sidx); free(slu); free(tdm); return 0; } lst[cnt++] = J; }
+    }
+    if (agg[i] >= 0) {
+      int q; for (q = 0; q < cnt; ++q) if (lst[q] == agg[i]) break;
+      if (q == cnt && cnt == P_ROW_MAX) { free(sidx); free(slu); free(tdm); return 0; }
+    }
+  }
   /* prolongation (make_prolomat semantics: first-appearance column order) */
   int *pidx = xc(n + 1, sizeof(int));
   int cap = sidx[n] + n;
@@ -793,6 +809,11 @@ static int own_coarsen(orc_t *o, int lv) {
       for (int q = pidx[j]; q < pidx[j + 1]; ++q) { tc[m] = pcol[q]; tv[m] = F->lumat[k] * pval[q]; m++; }
     }
     int u = accumulate_sorted(tc, tv, m, apcol + nap, apval + nap);
+    if (u > HASH_MAX) {
+      free(tc); free(tv); free(apidx); free(apcol); free(apval); free(pidx); free(pcol); free(pval);
+      free(ridx); free(rcol); free(rval);
+      return 0;
+    }
     nap += u; apidx[i + 1] = nap;
   }
   free(tc); free(tv);
@@ -815,6 +836,13 @@ static int own_coarsen(orc_t *o, int lv) {
       for (int a = apidx[i]; a < apidx[i + 1]; ++a) { tc[m] = apcol[a]; tv[m] = rval[q] * apval[a]; m++; }
     }
     int u = accumulate_sorted(tc, tv, m, oc, ov);
+    if (u > HASH_MAX) {
+      free(tc); free(tv); free(oc); free(ov); free(apidx); free(apcol); free(apval);
+      free(pidx); free(pcol); free(pval); free(ridx); free(rcol); free(rval);
+      free(C->offind); free(C->dmat); free(C->offrow); free(C->lumat);
+      memset(C, 0, sizeof(*C));
+      return 0;
+    }
     C->dmat[I] = DONE;
     for (int s = 0; s < u; ++s) {
       if (oc[s] == I) C->dmat[I] = ov[s];
@@ -840,7 +868,7 @@ static void own_amg_setup(orc_t *o) {
     o->nlevel++;
   }
   orc_level *Lc = &o->lev[o->nlevel - 1];
-  if (o->nlevel > 1) {
+  if (o->nlevel > 1 && Lc->n <= (o->prm.amg_coarse_max > 1 ? o->prm.amg_coarse_max : 1)) {
     Lc->cinv = xc((size_t)Lc->n * Lc->n, sizeof(double));
     dense_inverse(Lc, Lc->cinv);
   }

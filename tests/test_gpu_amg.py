@@ -1,0 +1,87 @@
+"""AMG on the GPU against the CPU oracle's restatement of the same algorithm.
+
+The setup (strength filter, MIS-2 aggregation, smoothed prolongation, R = P^T and
+the Galerkin product) is deterministic and fixes every summation order, so the
+hierarchy must match the oracle bit for bit; so must one V-cycle.
+"""
+import numpy as np
+import pytest
+
+from msg123_b200.config import make_config
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+AMG = dict(precon_type=1, ref_quirks=0, amg_coarse_max=200)
+
+
+def system(shape=(24, 20, 16), seed=6, delt=3600.0, **kw):
+    p = make_config("hetero", shape=shape, seed=seed, **kw)
+    o = Oracle(p, **AMG)
+    o.init_state()
+    o.set_state(head_new=p.head0 + 0.004 * np.random.default_rng(seed).standard_normal(p.ncalc), delt=delt)
+    d, lu, r = o.make_matvec()
+    return p, o, d, lu, r
+
+
+def gpu(p, **kw):
+    from msg123_b200.solver import GpuSolver
+    prm = dict(AMG)
+    prm.update(kw)
+    return GpuSolver(p, **prm)
+
+
+@pytest.mark.parametrize("shape,seed", [((24, 20, 16), 6), ((40, 36, 20), 8), ((9, 7, 5), 1)])
+def test_hierarchy_bitexact(shape, seed):
+    p, o, d, lu, r = system(shape, seed)
+    o.set_system(d, lu, r)
+    g = gpu(p)
+    g.set_system(d, lu, r)
+    lo, lg = o.amg_levels(), g.amg_levels()
+    assert len(lo) == len(lg) and len(lo) >= 2
+    for k in range(1, len(lo)):
+        a, b = lg[k], lo[k]
+        assert a["n"] == b["n"], k
+        for key in ("agg", "pindex", "poffrow", "offind", "offrow"):
+            assert np.array_equal(a[key], b[key]), (k, key)
+        for key in ("pval", "dmat", "lumat"):
+            assert np.array_equal(a[key], b[key]), (k, key)
+
+
+def test_vcycle_bitexact():
+    p, o, d, lu, r = system((32, 28, 18), 3)
+    o.set_system(d, lu, r)
+    g = gpu(p)
+    g.set_system(d, lu, r)
+    v = np.random.default_rng(5).standard_normal(p.ncalc)
+    zg, zo = g.precond(v), o.precond(v)
+    assert np.array_equal(zg, zo)
+
+
+def test_amg_bicgstab_counts():
+    p, o, d, lu, r = system((32, 28, 18), 3)
+    o2 = Oracle(p, maxinn_iter=100, **AMG)
+    o2.set_system(d, lu, r)
+    g = gpu(p, maxinn_iter=100)
+    g.set_system(d, lu, r)
+    b2 = float(r @ r)
+    xg, _, itg, cg = g.solve_linalg(b2, 1e-10)
+    xo, _, ito, co = o2.solve_linalg(b2, 1e-10)
+    assert itg == ito and cg == co == 1
+    assert np.max(np.abs(xg - xo)) <= 1e-9 * np.max(np.abs(xo))
+
+
+def test_amg_run_parity():
+    p = make_config("hetero", shape=(32, 28, 16), seed=12)
+    ov = dict(AMG, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    from msg123_b200.solver import GpuSolver
+    g, o = GpuSolver(p, **ov), Oracle(p, **ov)
+    g.init_state(); o.init_state()
+    rg, sg = g.advance(nsteps=3)
+    ro, so = o.advance(nsteps=3)
+    assert rg == ro == 0
+    hg, ho = g.get_state()["head_new"], o.get_state()["head_new"]
+    assert np.max(np.abs(hg - ho)) / np.max(np.abs(ho)) <= 1e-8
+    mg, mo = g.calc_mass(), o.calc_mass()
+    assert np.max(np.abs(mg - mo)) <= 1e-10 * abs(mo[2])
+    print("GPU", sg, "CPU", so)
