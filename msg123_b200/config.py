@@ -199,7 +199,7 @@ def make_hetero(shape=(256, 256, 64), d=(1.0, 1.0, 0.25), seed=2024, sigma=1.0, 
     rate = float(F32(rain_mm_h * 1.0e-3 / 3600.0) * lsi)
     rech = rate * np.full(nx * ny, ar)
     prm = default_params(len_scal=float(ls), criteria=1.0e-8, criteria_rel=1, lin_tol=0.0,
-                         maxinn_iter=100, precon_type=1, ref_quirks=0, sim_type=1, ini_step=600.0,
+                         maxinn_iter=100, precon_type=1, ref_quirks=0, amg_coarse_max=128, sim_type=1, ini_step=600.0,
                          max_step=3600.0, end_time=1.0e30)
     prm.update(pkw)
     p = Problem("hetero", nx, ny, nz, 0, 0, reta, nvg.astype(F32), np.full(N, 0.05, dtype=F32),

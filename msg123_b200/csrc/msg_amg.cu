@@ -108,16 +108,19 @@ __global__ void k_mis_init(int n, const int *has, int *st) {
 }
 
 // FROM_STATE: source tuples computed from st; else read from src.
-template <bool FROM_STATE>
-__global__ void k_mis_max(int n, const int *rowptr, const int *col, const unsigned char *sflag, const int *st,
-                          const unsigned long long *src, unsigned long long *dst, int lev) {
+__global__ void k_mis_tuple(int n, const int *st, unsigned long long *t0, int lev) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) t0[i] = mis_tuple(st[i], i, lev);
+}
+
+__global__ void k_mis_max(int n, const int *rowptr, const int *col, const unsigned char *sflag,
+                          const unsigned long long *src, unsigned long long *dst) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  unsigned long long m = FROM_STATE ? mis_tuple(st[i], i, lev) : src[i];
+  unsigned long long m = src[i];
   for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
     if (!sflag[k]) continue;
-    int j = col[k];
-    unsigned long long v = FROM_STATE ? mis_tuple(st[j], j, lev) : src[j];
+    unsigned long long v = src[col[k]];
     if (v > m) m = v;
   }
   dst[i] = m;
@@ -305,21 +308,30 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
                                                            const double *adiag, const int *bp, const int *bc,
                                                            const double *bv, int split_diag, int *ocnt,
                                                            const int *cptr, int *ccol, double *cval, double *cdiag,
-                                                           int *overflow) {
+                                                           int *overflow, const int *rows) {
   __shared__ int hk[kSpgWarps][kHash];
   __shared__ double hv[kSpgWarps][kHash];
   __shared__ int comp[kSpgWarps][kHashMax + 32];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int row = blockIdx.x * kSpgWarps + w;
-  if (row >= nrows) return;
+  int rid = blockIdx.x * kSpgWarps + w;
+  if (rid >= nrows) return;
+  const int row = rows ? rows[rid] : rid;
   int *K = hk[w];
   double *V = hv[w];
-  for (int t = lane; t < kHash; t += 32) { K[t] = -1; V[t] = 0.0; }
-  __syncwarp();
   int a0 = ap[row], a1 = ap[row + 1];
   int start = adiag ? a0 - 1 : a0;
-
-  bool ovf = false;
+  // products of this row -> table size (load factor <= 1/2 when it fits)
+  int m = 0;
+  for (int k = start + lane; k < a1; k += 32) {
+    int j = (k < a0) ? row : ac[k];
+    m += bp[j + 1] - bp[j];
+  }
+  for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+  int T = 32;
+  while (T < 2 * m && T < kHash) T <<= 1;
+  const unsigned mask = (unsigned)T - 1u;
+  for (int t = lane; t < T; t += 32) { K[t] = -1; V[t] = 0.0; }
+  __syncwarp();
   for (int k = start; k < a1; ++k) {
     int j;
     double coef;
@@ -329,58 +341,119 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
     for (int q = b0 + lane; q < b1; q += 32) {
       int cc = bc[q];
       double p = __dmul_rn(coef, bv[q]);
-      unsigned hsh = ((unsigned)cc * 2654435761u) & (kHash - 1);
-      for (int probe = 0; probe < kHash; ++probe) {
+      unsigned hsh = ((unsigned)cc * 2654435761u) & mask;
+      for (int probe = 0; probe < T; ++probe) {
         int cur = atomicCAS(&K[hsh], -1, cc);
         if (cur == -1 || cur == cc) { V[hsh] = __dadd_rn(V[hsh], p); break; }
-        hsh = (hsh + 1) & (kHash - 1);
+        hsh = (hsh + 1) & mask;
       }
     }
     __syncwarp();
   }
   // compact occupied slots
-  int m = 0;
-  for (int base = 0; base < kHash; base += 32) {
+  int u = 0;
+  for (int base = 0; base < T; base += 32) {
     int t = base + lane;
     bool occ = K[t] >= 0;
     unsigned bal = __ballot_sync(0xffffffffu, occ);
     if (occ) {
-      int pos = m + __popc(bal & ((1u << lane) - 1));
+      int pos = u + __popc(bal & ((1u << lane) - 1));
       if (pos < kHashMax + 32) comp[w][pos] = t;
     }
-    m += __popc(bal);
+    u += __popc(bal);
   }
   __syncwarp();
-  if (m > kHashMax) ovf = true;
-  if (ovf) {
+  if (u > kHashMax) {
     if (lane == 0) { atomicExch(overflow, 1); if (PASS == 0) ocnt[row] = 0; }
     return;
   }
   bool hasd = false;
   if (split_diag) {
-    for (int t = lane; t < m; t += 32) if (K[comp[w][t]] == row) hasd = true;
+    for (int t = lane; t < u; t += 32) if (K[comp[w][t]] == row) hasd = true;
     hasd = __any_sync(0xffffffffu, hasd);
   }
   if (PASS == 0) {
-    if (lane == 0) ocnt[row] = m - (hasd ? 1 : 0);
+    if (lane == 0) ocnt[row] = u - (hasd ? 1 : 0);
     return;
   }
   // rank sort by column
   int out0 = cptr[row];
   if (split_diag && lane == 0) cdiag[row] = 1.0;
   __syncwarp();
-  for (int t = lane; t < m; t += 32) {
+  for (int t = lane; t < u; t += 32) {
     int slot = comp[w][t];
     int key = K[slot];
     if (split_diag && key == row) { cdiag[row] = V[slot]; continue; }
     int rank = 0;
-    for (int u = 0; u < m; ++u) {
-      int k2 = K[comp[w][u]];
+    for (int v = 0; v < u; ++v) {
+      int k2 = K[comp[w][v]];
       if (split_diag && k2 == row) continue;
       rank += (k2 < key);
     }
     ccol[out0 + rank] = key;
     cval[out0 + rank] = V[slot];
+  }
+}
+
+
+// Thread-per-row variant for short rows (at most kTU distinct columns): the products
+// are summed one by one in generation order, exactly the CPU oracle's loop.  Rows
+// that need more columns are appended to `longrows` (PASS 0) or skipped (PASS 1)
+// and go through the warp kernel above.
+constexpr int kTU = 48, kTM = 64;
+template <int PASS>
+__global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, const int *ac, const double *av,
+                                                  const double *adiag, const int *bp, const int *bc, const double *bv,
+                                                  int split_diag, int *ocnt, const int *cptr, int *ccol, double *cval,
+                                                  double *cdiag, int *longrows, int *nlong) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nrows) return;
+  int uc[kTU];
+  double uv[kTU];
+  int u = 0;
+  int a0 = ap[row], a1 = ap[row + 1];
+  int m = 0;
+  for (int k = adiag ? a0 - 1 : a0; k < a1; ++k) {
+    int j = (k < a0) ? row : ac[k];
+    m += bp[j + 1] - bp[j];
+  }
+  if (m > kTM) {   // long product list: the warp kernel is faster
+    if (PASS == 0) longrows[atomicAdd(nlong, 1)] = row;
+    return;
+  }
+  for (int k = adiag ? a0 - 1 : a0; k < a1; ++k) {
+    int j = (k < a0) ? row : ac[k];
+    double coef = (k < a0) ? adiag[row] : av[k];
+    for (int q = bp[j]; q < bp[j + 1]; ++q) {
+      int cc = bc[q];
+      double p = __dmul_rn(coef, bv[q]);
+      int t = 0;
+      while (t < u && uc[t] != cc) ++t;
+      if (t < u) uv[t] = __dadd_rn(uv[t], p);
+      else if (u < kTU) { uc[u] = cc; uv[u] = p; ++u; }
+      else {
+        if (PASS == 0) { longrows[atomicAdd(nlong, 1)] = row; }
+        return;
+      }
+    }
+  }
+  // insertion sort by column
+  for (int a = 1; a < u; ++a) {
+    int c0 = uc[a]; double v0 = uv[a]; int b = a - 1;
+    while (b >= 0 && uc[b] > c0) { uc[b + 1] = uc[b]; uv[b + 1] = uv[b]; --b; }
+    uc[b + 1] = c0; uv[b + 1] = v0;
+  }
+  if (PASS == 0) {
+    int hasd = 0;
+    if (split_diag) for (int t = 0; t < u; ++t) hasd |= (uc[t] == row);
+    ocnt[row] = u - hasd;
+    return;
+  }
+  int o = cptr[row];
+  if (split_diag) cdiag[row] = 1.0;
+  for (int t = 0; t < u; ++t) {
+    if (split_diag && uc[t] == row) { cdiag[row] = uv[t]; continue; }
+    ccol[o] = uc[t]; cval[o] = uv[t]; ++o;
   }
 }
 
@@ -400,10 +473,16 @@ __global__ void k_dense_fill(int n, const int *rowptr, const int *col, const dou
   }
 }
 
-__global__ void __launch_bounds__(256) k_gj(int n, double *M, int *piv_out) {
-  cg::grid_group grid = cg::this_grid();
-  __shared__ double sa[256];
-  __shared__ int si[256];
+template <bool COOP, int NT>
+__global__ void __launch_bounds__(NT) k_gj(int n, double *M, int *piv_out) {
+  struct Sync {
+    __device__ void operator()() const {
+      if (COOP) cg::this_grid().sync();
+      else __syncthreads();
+    }
+  } sync_all;
+  __shared__ double sa[NT];
+  __shared__ int si[NT];
   const int w = 2 * n;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int p = 0; p < n; ++p) {
@@ -425,8 +504,8 @@ __global__ void __launch_bounds__(256) k_gj(int n, double *M, int *piv_out) {
       }
       if (threadIdx.x == 0) *piv_out = si[0];
     }
-    grid.sync();
-    int piv = *piv_out;
+    sync_all();
+    int piv = *(volatile int *)piv_out;
     // swap rows p and piv, then scale row p
     if (piv != p)
       for (int c = tid; c < w; c += nth) {
@@ -434,26 +513,28 @@ __global__ void __launch_bounds__(256) k_gj(int n, double *M, int *piv_out) {
         M[(size_t)p * w + c] = M[(size_t)piv * w + c];
         M[(size_t)piv * w + c] = t;
       }
-    grid.sync();
-    double pinv = __ddiv_rn(1.0, M[(size_t)p * w + p]);
-    grid.sync();
+    sync_all();
+    double pinv = __ddiv_rn(1.0, ((volatile double *)M)[(size_t)p * w + p]);
+    sync_all();
     for (int c = tid; c < w; c += nth) M[(size_t)p * w + c] = __dmul_rn(M[(size_t)p * w + c], pinv);
-    grid.sync();
-    // eliminate column p from every other row (factor read before the row changes)
-    for (size_t e = tid; e < (size_t)n * w; e += nth) {
-      int r = (int)(e / w), cc = (int)(e % w);
-      if (r == p) continue;
-      double f = M[(size_t)r * w + p];
-      if (f == 0.0 || cc == p) continue;
-      M[e] = __dsub_rn(M[e], __dmul_rn(f, M[(size_t)p * w + cc]));
-    }
-    grid.sync();
-    for (int r = tid; r < n; r += nth)
-      if (r != p) {
-        double f = M[(size_t)r * w + p];
-        if (f != 0.0) M[(size_t)r * w + p] = __dsub_rn(f, __dmul_rn(f, M[(size_t)p * w + p]));
+    sync_all();
+    // eliminate column p from every other row; the factor is read before the row
+    // changes (column p included: a_rp - f*a_pp, as the sequential loop computes it)
+    {
+      const int lane = threadIdx.x & 31;
+      const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+      const double *prow = M + (size_t)p * w;
+      for (int r = gw; r < n; r += nw) {
+        if (r == p) continue;
+        double *rrow = M + (size_t)r * w;
+        double f = rrow[p];
+        __syncwarp();
+        if (f == 0.0) continue;
+        for (int cc = lane; cc < w; cc += 32) rrow[cc] = __dsub_rn(rrow[cc], __dmul_rn(f, prow[cc]));
+        __syncwarp();
       }
-    grid.sync();
+    }
+    sync_all();
   }
 }
 
@@ -592,6 +673,59 @@ static int read_counter(msg_ctx *c, AmgState *A, int *v) {
   return MSG_OK;
 }
 
+
+// C = A*B (optionally with A's diagonal first, optionally splitting C's diagonal).
+// On return *cptr / *ccol / *cval (and cdiag) are allocated; *ovf set when a row
+// exceeds the warp kernel's table, in which case nothing is allocated.
+static int spgemm(msg_ctx *c, AmgState *A, int nrows, const int *ap, const int *ac, const double *av,
+                  const double *adiag, const int *bp, const int *bc, const double *bv, int split_diag, int **cptr,
+                  int **ccol, double **cval, double *cdiag, int *cnnz, int *ovf) {
+  cudaStream_t s = c->stream;
+  int rc;
+  int *cnt = nullptr, *longrows = nullptr, *nl = nullptr;
+  *ovf = 0;
+  if ((rc = dalloc(c, &cnt, nrows + 1))) return rc;
+  if ((rc = dalloc(c, &longrows, nrows + 1))) return rc;
+  if ((rc = dalloc(c, &nl, 2))) return rc;
+  MSG_CUDA(cudaMemsetAsync(nl, 0, 8, s));
+  k_spgemm_t<0><<<(nrows + 127) / 128, 128, 0, s>>>(nrows, ap, ac, av, adiag, bp, bc, bv, split_diag, cnt, nullptr,
+                                                   nullptr, nullptr, nullptr, longrows, nl);
+  MSG_CHECK_LAUNCH();
+  int h[2];
+  MSG_CUDA(cudaMemcpyAsync(h, nl, 8, cudaMemcpyDeviceToHost, s));
+  MSG_CUDA(cudaStreamSynchronize(s));
+  const int nlong = h[0];
+  MSG_CUDA(cudaMemsetAsync(A->cnt, 0, 4, s));
+  if (nlong > 0) {
+    k_spgemm<0><<<(nlong + kSpgWarps - 1) / kSpgWarps, 32 * kSpgWarps, 0, s>>>(
+        nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, cnt, nullptr, nullptr, nullptr, nullptr, A->cnt, longrows);
+    MSG_CHECK_LAUNCH();
+  }
+  if ((rc = dalloc(c, cptr, nrows + 1))) return rc;
+  int tot = 0;
+  if ((rc = scan_exclusive(c, cnt, *cptr, nrows, &tot))) return rc;
+  if ((rc = read_counter(c, A, ovf))) return rc;
+  if (*ovf) {
+    cudaFreeAsync(cnt, s); cudaFreeAsync(longrows, s); cudaFreeAsync(nl, s); cudaFreeAsync(*cptr, s);
+    *cptr = nullptr;
+    return MSG_OK;
+  }
+  MSG_CUDA(cudaMemcpyAsync(*cptr + nrows, &tot, 4, cudaMemcpyHostToDevice, s));
+  if ((rc = dalloc(c, ccol, tot))) return rc;
+  if ((rc = dalloc(c, cval, tot))) return rc;
+  k_spgemm_t<1><<<(nrows + 127) / 128, 128, 0, s>>>(nrows, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr,
+                                                   *ccol, *cval, cdiag, nullptr, nullptr);
+  MSG_CHECK_LAUNCH();
+  if (nlong > 0) {
+    k_spgemm<1><<<(nlong + kSpgWarps - 1) / kSpgWarps, 32 * kSpgWarps, 0, s>>>(
+        nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr, *ccol, *cval, cdiag, A->cnt, longrows);
+    MSG_CHECK_LAUNCH();
+  }
+  cudaFreeAsync(cnt, s); cudaFreeAsync(longrows, s); cudaFreeAsync(nl, s);
+  *cnnz = tot;
+  return MSG_OK;
+}
+
 // Build level lv+1 from level lv; returns 1 when a coarser level was made, 0 otherwise.
 static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   *made = 0;
@@ -611,16 +745,20 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   k_mis_init<<<nb(n), kThreads, 0, s>>>(n, A->has, A->st);
   MSG_CHECK_LAUNCH();
   for (int round = 0; round < 64; ++round) {
-    k_mis_max<true><<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->st, nullptr, A->t1, lv);
+    k_mis_tuple<<<nb(n), kThreads, 0, s>>>(n, A->st, A->t2, lv);
     MSG_CHECK_LAUNCH();
-    k_mis_max<false><<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->st, A->t1, A->t2, lv);
+    k_mis_max<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->t2, A->t1);
+    MSG_CHECK_LAUNCH();
+    k_mis_max<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->t1, A->t2);
     MSG_CHECK_LAUNCH();
     MSG_CUDA(cudaMemsetAsync(A->cnt, 0, 4, s));
     k_mis_update<<<nb(n), kThreads, 0, s>>>(n, A->st, A->t2, A->cnt);
     MSG_CHECK_LAUNCH();
-    int und = 0;
-    if ((rc = read_counter(c, A, &und))) return rc;
-    if (und == 0) break;
+    if ((round & 3) == 3 || round == 63) {   // a round with nothing undecided is a no-op
+      int und = 0;
+      if ((rc = read_counter(c, A, &und))) return rc;
+      if (und == 0) break;
+    }
   }
   k_root_flag<<<nb(n), kThreads, 0, s>>>(n, A->st, A->flag);
   MSG_CHECK_LAUNCH();
@@ -674,52 +812,20 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   // AP = A*P (diagonal first)
   int *apptr = nullptr, *apcol = nullptr;
   double *apval = nullptr;
-  int *cnt = nullptr;
-  if ((rc = dalloc(c, &cnt, std::max(n, nc) + 1))) return rc;
-  MSG_CUDA(cudaMemsetAsync(A->cnt, 0, 4, s));
-  int gw = (n + kSpgWarps - 1) / kSpgWarps;
-  k_spgemm<0><<<gw, 32 * kSpgWarps, 0, s>>>(n, F.rowptr, F.col, F.val, F.diag, C.pptr, C.pcol, C.pval, 0, cnt,
-                                            nullptr, nullptr, nullptr, nullptr, A->cnt);
-  MSG_CHECK_LAUNCH();
-  if ((rc = dalloc(c, &apptr, n + 1))) return rc;
-  int apn = 0;
-  if ((rc = scan_exclusive(c, cnt, apptr, n, &apn))) return rc;
-  int ovf = 0;
-  if ((rc = read_counter(c, A, &ovf))) return rc;
-  if (ovf) {
-    cudaFreeAsync(cnt, s); cudaFreeAsync(apptr, s);
-    free_level(C, s);
-    return MSG_OK;
-  }
-  MSG_CUDA(cudaMemcpyAsync(apptr + n, &apn, 4, cudaMemcpyHostToDevice, s));
-  if ((rc = dalloc(c, &apcol, apn))) return rc;
-  if ((rc = dalloc(c, &apval, apn))) return rc;
-  k_spgemm<1><<<gw, 32 * kSpgWarps, 0, s>>>(n, F.rowptr, F.col, F.val, F.diag, C.pptr, C.pcol, C.pval, 0, nullptr,
-                                            apptr, apcol, apval, nullptr, A->cnt);
-  MSG_CHECK_LAUNCH();
+  int apn = 0, ovf = 0;
+  if ((rc = spgemm(c, A, n, F.rowptr, F.col, F.val, F.diag, C.pptr, C.pcol, C.pval, 0, &apptr, &apcol, &apval,
+                   nullptr, &apn, &ovf)))
+    return rc;
+  if (ovf) { free_level(C, s); return MSG_OK; }
   // A_c = R * AP, diagonal split off
-  int gc = (nc + kSpgWarps - 1) / kSpgWarps;
-  k_spgemm<0><<<gc, 32 * kSpgWarps, 0, s>>>(nc, C.rptr, C.rcol, C.rval, nullptr, apptr, apcol, apval, 1, cnt,
-                                            nullptr, nullptr, nullptr, nullptr, A->cnt);
-  MSG_CHECK_LAUNCH();
-  if ((rc = dalloc(c, &C.rowptr, nc + 1))) return rc;
-  int cn = 0;
-  if ((rc = scan_exclusive(c, cnt, C.rowptr, nc, &cn))) return rc;
-  if ((rc = read_counter(c, A, &ovf))) return rc;
-  if (ovf) {
-    cudaFreeAsync(cnt, s); cudaFreeAsync(apptr, s); cudaFreeAsync(apcol, s); cudaFreeAsync(apval, s);
-    free_level(C, s);
-    return MSG_OK;
-  }
-  MSG_CUDA(cudaMemcpyAsync(C.rowptr + nc, &cn, 4, cudaMemcpyHostToDevice, s));
-  C.nnz = cn;
-  if ((rc = dalloc(c, &C.col, cn))) return rc;
-  if ((rc = dalloc(c, &C.val, cn))) return rc;
   if ((rc = dalloc(c, &C.diag, nc))) return rc;
-  k_spgemm<1><<<gc, 32 * kSpgWarps, 0, s>>>(nc, C.rptr, C.rcol, C.rval, nullptr, apptr, apcol, apval, 1, nullptr,
-                                            C.rowptr, C.col, C.val, C.diag, A->cnt);
-  MSG_CHECK_LAUNCH();
-  cudaFreeAsync(cnt, s); cudaFreeAsync(apptr, s); cudaFreeAsync(apcol, s); cudaFreeAsync(apval, s);
+  int cn = 0;
+  if ((rc = spgemm(c, A, nc, C.rptr, C.rcol, C.rval, nullptr, apptr, apcol, apval, 1, &C.rowptr, &C.col, &C.val,
+                   C.diag, &cn, &ovf)))
+    return rc;
+  cudaFreeAsync(apptr, s); cudaFreeAsync(apcol, s); cudaFreeAsync(apval, s);
+  if (ovf) { free_level(C, s); return MSG_OK; }
+  C.nnz = cn;
   if ((rc = dalloc(c, &C.x, nc))) return rc;
   if ((rc = dalloc(c, &C.b, nc))) return rc;
   if ((rc = dalloc(c, &C.r, nc))) return rc;
@@ -739,13 +845,19 @@ static int dense_inverse(msg_ctx *c, AmgLevel &L) {
   if ((rc = dalloc(c, &L.cinv, (size_t)n * n))) return rc;
   k_dense_fill<<<n, 256, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, M);
   MSG_CHECK_LAUNCH();
-  int per_sm = 0, sms = 0;
-  MSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj, 256, 0));
-  MSG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  int grid = std::max(1, std::min(sms * std::max(per_sm, 1), (n * 2 * n + 255) / 256));
-  void *args[] = {&n, &M, &piv};
-  MSG_CUDA(cudaLaunchCooperativeKernel((void *)k_gj, grid, 256, args, 0, s));
-  __atomic_fetch_add(&g_launches, 1LL, __ATOMIC_RELAXED);
+  if (n <= 1024) {
+    // one block: __syncthreads between the phases of a pivot step
+    k_gj<false, 1024><<<1, 1024, 0, s>>>(n, M, piv);
+    MSG_CHECK_LAUNCH();
+  } else {
+    int per_sm = 0, sms = 0;
+    MSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj<true, 256>, 256, 0));
+    MSG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    int grid = std::max(1, std::min(sms * std::max(per_sm, 1), (n * 2 * n + 255) / 256));
+    void *args[] = {&n, &M, &piv};
+    MSG_CUDA(cudaLaunchCooperativeKernel((void *)k_gj<true, 256>, grid, 256, args, 0, s));
+    __atomic_fetch_add(&g_launches, 1LL, __ATOMIC_RELAXED);
+  }
   k_dense_extract<<<n, 256, 0, s>>>(n, M, L.cinv);
   MSG_CHECK_LAUNCH();
   cudaFreeAsync(M, s);
@@ -824,35 +936,39 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
     if (l == 0) k_jac_dia<<<g, kThreads, 0, s>>>(D, b, w, xin, xout);
     else k_jac_csr<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, b, w, xin, xout);
   };
-  // pre-smoothing
+  // pre-smoothing: the current iterate alternates between x and tmp, so that every
+  // sweep reads one buffer and writes the other; total sweeps 2*sw end in x.
+  double *cur = x, *oth = tmp;
   if (sw == 0) {
     MSG_CUDA(cudaMemsetAsync(x, 0, (size_t)n * 8, s));
   } else {
-    k_jac_first<<<g, kThreads, 0, s>>>(n, b, l == 0 ? c->dmat : L.diag, w, x);
+    if (sw % 2 == 0) { cur = tmp; oth = x; }
+    k_jac_first<<<g, kThreads, 0, s>>>(n, b, l == 0 ? c->dmat : L.diag, w, cur);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      sweep(x, tmp);
+      sweep(cur, oth);
       MSG_CHECK_LAUNCH();
-      MSG_CUDA(cudaMemcpyAsync(x, tmp, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+      std::swap(cur, oth);
     }
   }
   if (!last) {
     AmgLevel &C = A->lv[l + 1];
-    if (l == 0) k_res_dia<<<g, kThreads, 0, s>>>(D, b, x, r);
-    else k_res_csr<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, b, x, r);
+    if (l == 0) k_res_dia<<<g, kThreads, 0, s>>>(D, b, cur, r);
+    else k_res_csr<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, b, cur, r);
     MSG_CHECK_LAUNCH();
     k_restrict<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval, r, C.b);
     MSG_CHECK_LAUNCH();
     int rc = vcycle(c, l + 1, C.b, C.x);
     if (rc) return rc;
-    k_prolong<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval, C.x, x);
+    k_prolong<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval, C.x, cur);
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {
-    sweep(x, tmp);
+    sweep(cur, oth);
     MSG_CHECK_LAUNCH();
-    MSG_CUDA(cudaMemcpyAsync(x, tmp, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    std::swap(cur, oth);
   }
+  if (cur != x) MSG_CUDA(cudaMemcpyAsync(x, cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
   return MSG_OK;
 }
 

@@ -404,6 +404,14 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
   c->delt = p->ini_step; c->delt_inv = 1.0 / p->ini_step;
   c->last_conv = -1;
   MSG_CUDA(cudaGetDevice(&c->device));
+  {
+    // keep freed stream-ordered allocations in the pool (the AMG hierarchy is rebuilt
+    // every Newton iteration; returning memory to the OS at each sync costs ~ms)
+    cudaMemPool_t pool;
+    MSG_CUDA(cudaDeviceGetDefaultMemPool(&pool, c->device));
+    uint64_t thr = UINT64_MAX;
+    MSG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  }
   MSG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (int k = 0; k < 8; ++k) MSG_CUDA(cudaEventCreate(&c->ev[k]));
   // symmetric face areas are required by the face-shared DIA storage
