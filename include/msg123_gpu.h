@@ -80,7 +80,7 @@ typedef struct msg_params {
   float amg_theta;           /* strength threshold (real(SP))                                          */
   float smooth_omega;        /* Jacobi smoother weight                                                */
   int32_t sim_type;          /* 0: delt*inc_fact per accepted step; 1: heuristic (apply_heuri)         */
-  int32_t pad1;
+  int32_t amg_lag;           /* 0: AMG rebuilt at every make_matvec (reference); 1: once per time step */
   double ini_step;           /* initial delt (s)                                                      */
   double inc_fact;           /* factor for sim_type 0                                                 */
   double max_step;           /* cap on delt for sim_type 1                                            */
@@ -205,6 +205,12 @@ MSG_API int msg_gpu_amg_nlevel(msg_ctx_t *ctx);
 MSG_API int msg_gpu_amg_level_sizes(msg_ctx_t *ctx, int32_t lv, int32_t *n, int32_t *nnz, int32_t *pnnz);
 MSG_API int msg_gpu_amg_level(msg_ctx_t *ctx, int32_t lv, int32_t *offind, int32_t *offrow, double *dmat,
                               double *lumat, int32_t *pindex, int32_t *poffrow, double *pval, int32_t *agg);
+
+/* Dense FP64 inverse by Gauss-Jordan with partial pivoting (ties to the lowest row):
+ * the coarsest-level solve of the AMG V-cycle (the reference's coarsest level is
+ * smoothed by solve_ilu instead, Linear_solution.f90:617-660).  a and inv are host
+ * arrays, row-major n x n.  Allocates its device buffers. */
+MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv);
 
 /* Number of kernels this library has launched in this process (all contexts). */
 MSG_API long long msg_gpu_launch_count(void);

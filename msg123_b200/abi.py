@@ -49,7 +49,7 @@ class MsgParams(C.Structure):
         ("precon_type", C.c_int32), ("ref_quirks", C.c_int32), ("precision", C.c_int32),
         ("amg_nlevel", C.c_int32), ("amg_coarse_max", C.c_int32), ("amg_sweeps", C.c_int32),
         ("jac_omega", C.c_float), ("amg_theta", C.c_float), ("smooth_omega", C.c_float),
-        ("sim_type", C.c_int32), ("pad1", C.c_int32),
+        ("sim_type", C.c_int32), ("amg_lag", C.c_int32),
         ("ini_step", C.c_double), ("inc_fact", C.c_double), ("max_step", C.c_double),
         ("end_time", C.c_double),
     ]

@@ -538,6 +538,14 @@ __global__ void __launch_bounds__(NT) k_gj(int n, double *M, int *piv_out) {
   }
 }
 
+// [A | I] from a dense row-major matrix
+__global__ void k_dense_fill_rm(int n, const double *a, double *M) {
+  int i = blockIdx.x;
+  int w = 2 * n;
+  for (int c = threadIdx.x; c < w; c += blockDim.x)
+    M[(size_t)i * w + c] = (c < n) ? a[(size_t)i * n + c] : ((c == n + i) ? 1.0 : 0.0);
+}
+
 __global__ void k_dense_extract(int n, const double *M, double *inv) {
   int i = blockIdx.x;
   for (int j = threadIdx.x; j < n; j += blockDim.x) inv[(size_t)i * n + j] = M[(size_t)i * 2 * n + n + j];
@@ -982,6 +990,41 @@ int amg_apply(msg_ctx *c, const double *r, double *z) {
 // Hierarchy export for structural tests (levels are 0-based; level 0 is the Jacobian).
 using namespace msg;
 extern "C" {
+// Dense FP64 inverse by Gauss-Jordan with partial pivoting: the coarsest-level
+// solve of the AMG V-cycle, on host arrays (row-major n x n).
+MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv) {
+  if (n < 1 || !a || !inv) { set_error("dense_inverse: bad arguments"); return MSG_ERR_ARG; }
+  double *da = nullptr, *M = nullptr, *dinv = nullptr;
+  int *piv = nullptr;
+  const size_t nn = (size_t)n * n;
+  MSG_CUDA(cudaMalloc(&da, nn * 8));
+  MSG_CUDA(cudaMalloc(&M, 2 * nn * 8));
+  MSG_CUDA(cudaMalloc(&dinv, nn * 8));
+  MSG_CUDA(cudaMalloc(&piv, 4));
+  MSG_CUDA(cudaMemcpy(da, a, nn * 8, cudaMemcpyHostToDevice));
+  k_dense_fill_rm<<<n, 256>>>(n, da, M);
+  MSG_CHECK_LAUNCH();
+  if (n <= 1024) {
+    k_gj<false, 1024><<<1, 1024>>>(n, M, piv);
+    MSG_CHECK_LAUNCH();
+  } else {
+    int dev = 0, per_sm = 0, sms = 0;
+    MSG_CUDA(cudaGetDevice(&dev));
+    MSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj<true, 256>, 256, 0));
+    MSG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int grid = std::max(1, std::min(sms * std::max(per_sm, 1), (int)((2 * nn + 255) / 256)));
+    int nn32 = n;
+    void *args[] = {&nn32, &M, &piv};
+    MSG_CUDA(cudaLaunchCooperativeKernel((void *)k_gj<true, 256>, grid, 256, args, 0, 0));
+    __atomic_fetch_add(&g_launches, 1LL, __ATOMIC_RELAXED);
+  }
+  k_dense_extract<<<n, 256>>>(n, M, dinv);
+  MSG_CHECK_LAUNCH();
+  MSG_CUDA(cudaMemcpy(inv, dinv, nn * 8, cudaMemcpyDeviceToHost));
+  cudaFree(da); cudaFree(M); cudaFree(dinv); cudaFree(piv);
+  return MSG_OK;
+}
+
 MSG_API int msg_gpu_amg_nlevel(msg_ctx_t *c) {
   return (c && S(c)) ? (int)S(c)->lv.size() : 0;
 }

@@ -81,7 +81,9 @@ static int make_matvec(msg_ctx *c, double *l2_rhs) {
   if (l2_rhs) *l2_rhs = s;
   if (c->timing) cudaEventRecord(ev[1], c->stream);
   if (c->prm.precon_type == 1 && !c->prm.ref_quirks) {
-    if ((rc = amg_setup(c))) return rc;
+    // amg_lag = 1 keeps the hierarchy of the time step's first Newton iteration
+    if (!c->prm.amg_lag || c->out_iter <= 1 || c->amg_nlevel <= 1)
+      if ((rc = amg_setup(c))) return rc;
   }
   if (c->timing) {
     cudaEventRecord(ev[2], c->stream);
@@ -579,6 +581,7 @@ int msg_gpu_calc_func(msg_ctx_t *c, const double *infx, double *funcv) {
 
 int msg_gpu_make_matvec(msg_ctx_t *c, double *dmat, double *lumat, double *rhs) {
   if (!c) return MSG_ERR_ARG;
+  c->out_iter = 0;   // a direct call always rebuilds the hierarchy
   double l2;
   int rc = make_matvec(c, &l2);
   if (rc) return rc;

@@ -65,6 +65,7 @@ def load_library():
     L.msg_gpu_amg_nlevel.argtypes = [vp]
     L.msg_gpu_amg_level_sizes.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PI]
     L.msg_gpu_amg_level.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
+    L.msg_gpu_dense_inverse.argtypes = [C.c_int32, abi.PD, abi.PD]
     L.msg_gpu_launch_count.restype = C.c_longlong
     L.msg_gpu_launch_count.argtypes = []
     _lib = L
@@ -73,6 +74,15 @@ def load_library():
 
 def launch_count():
     return int(load_library().msg_gpu_launch_count())
+
+
+def dense_inverse(a):
+    """Inverse of a dense square matrix (the AMG coarsest-level solve) on the GPU."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    inv = np.zeros((n, n))
+    _check(load_library().msg_gpu_dense_inverse(n, dptr(a), dptr(inv)), "dense_inverse")
+    return inv
 
 
 def _check(rc, what):

@@ -448,7 +448,7 @@ static void make_matvec(orc_t *o) {
   make_matrix(o, o->lev[0].dmat, o->lev[0].lumat);
   if (o->prm.precon_type == 1) {
     if (o->prm.ref_quirks) make_amgmat(o);
-    else own_amg_setup(o);
+    else if (!o->prm.amg_lag || o->out_iter <= 1 || o->nlevel <= 1) own_amg_setup(o);
   }
   free(tmp);
 }
@@ -615,14 +615,13 @@ static void free_level(orc_level *L) {
   memset(L, 0, sizeof(*L));
 }
 
-/* Gauss-Jordan inverse with partial pivoting (ties: smallest row), row-major. */
-static void dense_inverse(const orc_level *L, double *inv) {
-  int n = L->n;
-  double *a = xc((size_t)n * 2 * n, sizeof(double));
+/* Gauss-Jordan inverse with partial pivoting (ties: smallest row) of a dense
+ * row-major n x n matrix; the augmented [A | I] is reduced in place. */
+static void dense_inverse_rm(int n, const double *A, double *inv) {
   int w = 2 * n;
+  double *a = xc((size_t)n * w, sizeof(double));
   for (int i = 0; i < n; ++i) {
-    a[(size_t)i * w + i] = L->dmat[i];
-    for (int k = L->offind[i]; k < L->offind[i + 1]; ++k) a[(size_t)i * w + L->offrow[k]] = L->lumat[k];
+    for (int j = 0; j < n; ++j) a[(size_t)i * w + j] = A[(size_t)i * n + j];
     a[(size_t)i * w + n + i] = DONE;
   }
   for (int p = 0; p < n; ++p) {
@@ -640,6 +639,17 @@ static void dense_inverse(const orc_level *L, double *inv) {
   }
   for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) inv[(size_t)i * n + j] = a[(size_t)i * w + n + j];
   free(a);
+}
+
+static void dense_inverse(const orc_level *L, double *inv) {
+  int n = L->n;
+  double *A = xc((size_t)n * n, sizeof(double));
+  for (int i = 0; i < n; ++i) {
+    A[(size_t)i * n + i] = L->dmat[i];
+    for (int k = L->offind[i]; k < L->offind[i + 1]; ++k) A[(size_t)i * n + L->offrow[k]] = L->lumat[k];
+  }
+  dense_inverse_rm(n, A, inv);
+  free(A);
 }
 
 /* Accumulate (col,val) products in generation order into unique columns; returns
@@ -1354,6 +1364,7 @@ void orc_calc_func(void *h, const double *x, double *f) { calc_func((orc_t *)h, 
 
 void orc_make_matvec(void *h, double *dmat, double *lumat, double *rhs) {
   orc_t *o = h;
+  o->out_iter = 0;   /* a direct call always rebuilds the hierarchy */
   make_matvec(o);
   if (dmat) memcpy(dmat, o->lev[0].dmat, 8 * o->ncalc);
   if (lumat) memcpy(lumat, o->lev[0].lumat, 8 * o->nnz);
@@ -1424,6 +1435,8 @@ void orc_amg_level(void *h, int lv, int *offind, int *offrow, double *dmat, doub
     if (agg && g_last_agg[lv - 1]) memcpy(agg, g_last_agg[lv - 1], sizeof(int) * nf);
   }
 }
+void orc_dense_inverse(int n, const double *a, double *inv) { dense_inverse_rm(n, a, inv); }
+
 long long orc_counter(void *h, int which) {
   orc_t *o = h; return which == 0 ? o->n_func : which == 1 ? o->n_matvec : o->n_prec;
 }

@@ -54,6 +54,14 @@ def lib():
     return _lib
 
 
+def dense_inverse(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    inv = np.zeros((n, n))
+    lib().orc_dense_inverse(C.c_int(n), dptr(a), dptr(inv))
+    return inv
+
+
 class Oracle:
     """CPU oracle instance for one Problem (msg123_b200.config.Problem)."""
 
