@@ -212,6 +212,16 @@ MSG_API int msg_gpu_amg_level(msg_ctx_t *ctx, int32_t lv, int32_t *offind, int32
  * arrays, row-major n x n.  Allocates its device buffers. */
 MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv);
 
+/* Allocation-free variant of msg_gpu_dense_inverse, for callers that cannot call
+ * cudaMalloc (a host that passes device arrays it already owns, or a step running
+ * under a fixed device-memory budget).  No counterpart exists in the reference.
+ * a_dev / inv_dev: caller-owned device arrays, row-major n x n, 1 <= n <= 512 (larger n
+ * returns MSG_ERR_SIZE).  Work is queued on `stream` (NULL: legacy default stream).
+ * The workspace is one static device array per GPU (about 4 MiB, held until exit);
+ * the first call on a device looks up its address and should precede any stream
+ * capture; concurrent calls on one device race on that workspace. */
+MSG_API int msg_gpu_dense_inverse_noalloc(int32_t n, const double *a_dev, double *inv_dev, void *stream);
+
 /* Number of kernels this library has launched in this process (all contexts). */
 MSG_API long long msg_gpu_launch_count(void);
 

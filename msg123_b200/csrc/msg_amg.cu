@@ -18,6 +18,7 @@
 #include <cuda_bf16.h>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 namespace cg = cooperative_groups;
 
@@ -987,6 +988,45 @@ int amg_apply(msg_ctx *c, const double *r, double *z) {
 
 }  // namespace msg
 
+
+// ---------------------------------------------------------------------------------
+// Allocation-free dense inverse.
+//
+// Some callers cannot call cudaMalloc: a Fortran host that hands over device arrays it
+// already owns (CUDA Fortran or OpenACC data regions) while its own allocator holds the
+// device heap, or a solver step that runs under a fixed device-memory budget where an
+// allocation could fail or stall mid-step.  msg_gpu_dense_inverse_noalloc serves them:
+// it takes the caller's device buffers and keeps its Gauss-Jordan workspace (the
+// augmented [A | I] block and the pivot slot) in the file-scope array below, sized for
+// n <= kNoAllocMaxN.  Every GPU that loads this library holds that array (about 4 MiB)
+// until the process exits.
+// ---------------------------------------------------------------------------------
+constexpr int kNoAllocMaxN = 512;
+static __device__ __align__(256) double g_noalloc_gj[(size_t)2 * kNoAllocMaxN * kNoAllocMaxN + 32];
+
+static double *g_noalloc_addr[64];   // device address of g_noalloc_gj, per device (host side)
+static std::mutex g_noalloc_mu;
+
+// In host code g_noalloc_gj names a host-side stand-in, not device memory: the device
+// address must come from cudaGetSymbolAddress, once per device, with that device current.
+static int noalloc_scratch(double **out) {
+  int dev = 0;
+  MSG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { ::msg::set_error("dense_inverse_noalloc: device %d out of range", dev); return MSG_ERR_ARG; }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_gj);
+    if (e != cudaSuccess || !p) {
+      ::msg::set_error("dense_inverse_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return MSG_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return MSG_OK;
+}
+
 // Hierarchy export for structural tests (levels are 0-based; level 0 is the Jacobian).
 using namespace msg;
 extern "C" {
@@ -1022,6 +1062,33 @@ MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv) {
   MSG_CHECK_LAUNCH();
   MSG_CUDA(cudaMemcpy(inv, dinv, nn * 8, cudaMemcpyDeviceToHost));
   cudaFree(da); cudaFree(M); cudaFree(dinv); cudaFree(piv);
+  return MSG_OK;
+}
+
+// Same result as msg_gpu_dense_inverse, bit for bit, without any allocation: a_dev and
+// inv_dev are device arrays (row-major n x n) owned by the caller; the work runs on
+// `stream` (NULL: the legacy default stream) and is complete when that stream is.
+// The first call on a device looks up the scratch address (cudaGetSymbolAddress); make
+// that first call before any stream capture.  All calls share one workspace per device,
+// so calls that overlap on the GPU race; each call writes the whole [A | I] block and
+// the pivot slot before reading them, so nothing needs to start at zero.
+MSG_API int msg_gpu_dense_inverse_noalloc(int32_t n, const double *a_dev, double *inv_dev, void *stream) {
+  if (n < 1 || n > kNoAllocMaxN) {
+    set_error("dense_inverse_noalloc: n = %d outside 1..%d (workspace limit)", (int)n, kNoAllocMaxN);
+    return MSG_ERR_SIZE;
+  }
+  if (!a_dev || !inv_dev) { set_error("dense_inverse_noalloc: null device pointer"); return MSG_ERR_ARG; }
+  double *M = nullptr;
+  int rc = noalloc_scratch(&M);
+  if (rc) return rc;
+  int *piv = reinterpret_cast<int *>(M + (size_t)2 * kNoAllocMaxN * kNoAllocMaxN);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_dense_fill_rm<<<n, 256, 0, s>>>(n, a_dev, M);
+  MSG_CHECK_LAUNCH();
+  k_gj<false, 1024><<<1, 1024, 0, s>>>(n, M, piv);
+  MSG_CHECK_LAUNCH();
+  k_dense_extract<<<n, 256, 0, s>>>(n, M, inv_dev);
+  MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
 
