@@ -85,6 +85,9 @@ typedef struct msg_params {
   double inc_fact;           /* factor for sim_type 0                                                 */
   double max_step;           /* cap on delt for sim_type 1                                            */
   double end_time;           /* simulation end (s)                                                    */
+  int32_t guess_mode;        /* Newton initial guess: 0 = previous head (reference), 1 = linear
+                                extrapolation, 2 = learned increment (extrapolation on failure)      */
+  int32_t pad2;
 } msg_params_t;
 
 /* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */

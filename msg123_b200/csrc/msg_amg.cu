@@ -52,6 +52,7 @@ struct AmgState {
   size_t cap_n = 0;              // scratch capacity (rows)
   size_t sflag_cap = 0;
   double *r0 = nullptr, *t0 = nullptr;   // level-1 V-cycle work vectors
+  float *x0f = nullptr, *t0f = nullptr, *r0f = nullptr;   // level-1 FP32 work vectors (precision = 1)
   // setup scratch
   unsigned char *sflag = nullptr;
   int *has = nullptr, *st = nullptr, *flag = nullptr, *aggid = nullptr, *agg2 = nullptr, *tmpi = nullptr;
@@ -632,6 +633,98 @@ __global__ void k_gemv(int n, const double *Ci, const double *b, double *x) {
   x[i] = s;
 }
 
+
+// ---------------------------------------------------------------------------------
+// Mixed-precision V-cycle (precision = 1): FP32 vectors, FP32 level-1 operator and
+// transfer weights, BF16 off-diagonals and FP32 diagonal on the coarse levels, FP64
+// dense inverse at the coarsest level.  The Krylov recurrences stay FP64: the input r
+// is read as double and the output z written as double.
+// ---------------------------------------------------------------------------------
+struct Dia32 {
+  int nx, ny, nz, nxy, N;
+  const float *d, *lu;
+};
+
+__device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x) {
+  int iz = i / A.nxy, rem = i - iz * A.nxy, iy = rem / A.nx, ix = rem - iy * A.nx;
+  const size_t N = A.N;
+  float t = A.d[i] * x[i];
+  if (iz > 0) t += A.lu[0 * N + i] * x[i - A.nxy];
+  if (iy > 0) t += A.lu[1 * N + i] * x[i - A.nx];
+  if (ix > 0) t += A.lu[2 * N + i] * x[i - 1];
+  if (ix < A.nx - 1) t += A.lu[3 * N + i] * x[i + 1];
+  if (iy < A.ny - 1) t += A.lu[4 * N + i] * x[i + A.nx];
+  if (iz < A.nz - 1) t += A.lu[5 * N + i] * x[i + A.nxy];
+  return t;
+}
+
+__device__ __forceinline__ float csr_row_h(int i, const int *rp, const int *cl, const __nv_bfloat16 *v,
+                                           const float *d, const float *x) {
+  float t = d[i] * x[i];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) t += __bfloat162float(v[k]) * x[cl[k]];
+  return t;
+}
+
+template <typename TB>
+__global__ void k_jac_first_f(int n, const TB *b, const float *d, float w, float *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = (w * (float)b[i]) / d[i];
+}
+template <typename TY>
+__global__ void k_jac_dia_f(Dia32 A, const double *b, float w, const float *x, TY *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x) {
+    float r = (float)b[i] - dia_row_f(A, i, x);
+    y[i] = (TY)(x[i] + (w * r) / A.d[i]);
+  }
+}
+__global__ void k_res_dia_f(Dia32 A, const double *b, const float *x, float *r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x)
+    r[i] = (float)b[i] - dia_row_f(A, i, x);
+}
+__global__ void k_jac_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
+                            const float *b, float w, const float *x, float *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float r = b[i] - csr_row_h(i, rp, cl, v, d, x);
+    y[i] = x[i] + (w * r) / d[i];
+  }
+}
+__global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
+                            const float *b, const float *x, float *r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r[i] = b[i] - csr_row_h(i, rp, cl, v, d, x);
+}
+__global__ void k_restrict_f(int nc, const int *rp, const int *rc, const float *rv, const float *r, float *bc) {
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int q = rp[I]; q < rp[I + 1]; ++q) s += rv[q] * r[rc[q]];
+    bc[I] = s;
+  }
+}
+__global__ void k_prolong_f(int nf, const int *pp, const int *pc, const float *pv, const float *xc, float *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int q = pp[i]; q < pp[i + 1]; ++q) s += pv[q] * xc[pc[q]];
+    x[i] += s;
+  }
+}
+// coarsest level: FP64 dense inverse applied to a float right-hand side
+__global__ void k_gemv_mixed(int n, const double *Ci, const float *b, float *x) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < n; ++j) s += Ci[(size_t)i * n + j] * (double)b[j];
+  x[i] = (float)s;
+}
+__global__ void k_d2f(int n, const double *a, float *b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+__global__ void k_d2h(int n, const double *a, __nv_bfloat16 *b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = __double2bfloat16(a[i]);
+}
+__global__ void k_f2d(int n, const float *a, double *b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (double)a[i];
+}
+
 __global__ void k_col0(int nnz, const int *offrow1, int *col0) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < nnz) col0[k] = offrow1[k] - 1;
@@ -880,7 +973,7 @@ void amg_free(msg_ctx *c) {
   cudaStream_t s = c->stream;
   for (size_t l = 1; l < A->lv.size(); ++l) free_level(A->lv[l], s);
   A->lv.clear();
-  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t1, A->t2,
+  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t1, A->t2,
                A->tdm, A->d1f, A->lu1f};
   for (void *q : p) if (q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
@@ -901,6 +994,11 @@ int amg_setup(msg_ctx *c) {
     if ((rc = dalloc(c, &A->cnt, 1))) return rc;
     if ((rc = dalloc(c, &A->r0, c->N))) return rc;
     if ((rc = dalloc(c, &A->t0, c->N))) return rc;
+    if (c->prm.precision == 1) {
+      if ((rc = dalloc(c, &A->x0f, c->N))) return rc;
+      if ((rc = dalloc(c, &A->t0f, c->N))) return rc;
+      if ((rc = dalloc(c, &A->r0f, c->N))) return rc;
+    }
     MSG_CUDA(cudaMallocHost((void **)&A->hcnt, 4));
     k_col0<<<nb(c->nnz), kThreads, 0, s>>>(c->nnz, c->offrow, A->col0);
     MSG_CHECK_LAUNCH();
@@ -919,6 +1017,29 @@ int amg_setup(msg_ctx *c) {
   }
   if (A->lv.size() > 1 && A->lv.back().n <= std::max(c->prm.amg_coarse_max, 1)) {
     if ((rc = dense_inverse(c, A->lv.back()))) return rc;
+  }
+  if (c->prm.precision == 1) {
+    for (size_t l = 1; l < A->lv.size(); ++l) {
+      AmgLevel &L = A->lv[l];
+      int nf = A->lv[l - 1].n;
+      if ((rc = dalloc(c, &L.diag_f, L.n))) return rc;
+      if ((rc = dalloc(c, &L.val_h, L.nnz))) return rc;
+      if ((rc = dalloc(c, &L.pval_f, L.pnnz))) return rc;
+      if ((rc = dalloc(c, &L.rval_f, L.pnnz))) return rc;
+      if ((rc = dalloc(c, &L.xf, L.n))) return rc;
+      if ((rc = dalloc(c, &L.bf, L.n))) return rc;
+      if ((rc = dalloc(c, &L.rf, L.n))) return rc;
+      if ((rc = dalloc(c, &L.x2f, L.n))) return rc;
+      int g = std::min(nb(std::max(L.nnz, L.pnnz)), kRedBlocks * 4);
+      k_d2f<<<std::min(nb(L.n), kRedBlocks * 4), kThreads, 0, s>>>(L.n, L.diag, L.diag_f);
+      MSG_CHECK_LAUNCH();
+      if (L.nnz) { k_d2h<<<g, kThreads, 0, s>>>(L.nnz, L.val, L.val_h); MSG_CHECK_LAUNCH(); }
+      k_d2f<<<g, kThreads, 0, s>>>(L.pnnz, L.pval, L.pval_f);
+      MSG_CHECK_LAUNCH();
+      k_d2f<<<g, kThreads, 0, s>>>(L.pnnz, L.rval, L.rval_f);
+      MSG_CHECK_LAUNCH();
+      (void)nf;
+    }
   }
   c->amg_nlevel = (int)A->lv.size();
   return MSG_OK;
@@ -981,8 +1102,104 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
   return MSG_OK;
 }
 
+
+// Mixed-precision V-cycle on levels >= 1 (float vectors).
+static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
+  AmgState *A = S(c);
+  AmgLevel &L = A->lv[l];
+  cudaStream_t s = c->stream;
+  const int n = L.n, sw = std::max(c->prm.amg_sweeps, 0);
+  const float w = c->prm.smooth_omega;
+  const int g = std::min(nb(n), kRedBlocks * 4);
+  const bool last = (l == (int)A->lv.size() - 1);
+  if (last && L.cinv) {
+    k_gemv_mixed<<<nb(n), kThreads, 0, s>>>(n, L.cinv, b, x);
+    MSG_CHECK_LAUNCH();
+    return MSG_OK;
+  }
+  float *cur = x, *oth = L.x2f;
+  if (sw == 0) {
+    MSG_CUDA(cudaMemsetAsync(x, 0, (size_t)n * 4, s));
+  } else {
+    if (sw % 2 == 0) { cur = L.x2f; oth = x; }
+    k_jac_first_f<float><<<g, kThreads, 0, s>>>(n, b, L.diag_f, w, cur);
+    MSG_CHECK_LAUNCH();
+    for (int k = 1; k < sw; ++k) {
+      k_jac_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+      MSG_CHECK_LAUNCH();
+      std::swap(cur, oth);
+    }
+  }
+  if (!last) {
+    AmgLevel &C = A->lv[l + 1];
+    k_res_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
+    MSG_CHECK_LAUNCH();
+    k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
+    MSG_CHECK_LAUNCH();
+    int rc = vcycle_f(c, l + 1, C.bf, C.xf);
+    if (rc) return rc;
+    k_prolong_f<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
+    MSG_CHECK_LAUNCH();
+  }
+  for (int k = 0; k < sw; ++k) {
+    k_jac_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+    MSG_CHECK_LAUNCH();
+    std::swap(cur, oth);
+  }
+  if (cur != x) MSG_CUDA(cudaMemcpyAsync(x, cur, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  return MSG_OK;
+}
+
+// Level 1 of the mixed V-cycle: r (FP64 Krylov vector) in, z (FP64) out.
+static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
+  AmgState *A = S(c);
+  cudaStream_t s = c->stream;
+  const int n = c->N, sw = std::max(c->prm.amg_sweeps, 0);
+  const float w = c->prm.smooth_omega;
+  const int g = std::min(nb(n), kRedBlocks * 4);
+  Dia32 D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, c->lu_f};
+  const bool single = (A->lv.size() == 1);
+  float *cur = A->x0f, *oth = A->t0f;
+  if (sw == 0) {
+    MSG_CUDA(cudaMemsetAsync(cur, 0, (size_t)n * 4, s));
+  } else {
+    k_jac_first_f<double><<<g, kThreads, 0, s>>>(n, b, c->dmat_f, w, cur);
+    MSG_CHECK_LAUNCH();
+    for (int k = 1; k < sw; ++k) {
+      k_jac_dia_f<float><<<g, kThreads, 0, s>>>(D, b, w, cur, oth);
+      MSG_CHECK_LAUNCH();
+      std::swap(cur, oth);
+    }
+  }
+  if (!single) {
+    AmgLevel &C = A->lv[1];
+    k_res_dia_f<<<g, kThreads, 0, s>>>(D, b, cur, A->r0f);
+    MSG_CHECK_LAUNCH();
+    k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
+    MSG_CHECK_LAUNCH();
+    int rc = vcycle_f(c, 1, C.bf, C.xf);
+    if (rc) return rc;
+    k_prolong_f<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
+    MSG_CHECK_LAUNCH();
+  }
+  for (int k = 0; k < sw; ++k) {
+    if (k == sw - 1) {   // the last sweep writes the FP64 output
+      k_jac_dia_f<double><<<g, kThreads, 0, s>>>(D, b, w, cur, z);
+      MSG_CHECK_LAUNCH();
+      return MSG_OK;
+    }
+    k_jac_dia_f<float><<<g, kThreads, 0, s>>>(D, b, w, cur, oth);
+    MSG_CHECK_LAUNCH();
+    std::swap(cur, oth);
+  }
+  k_f2d<<<g, kThreads, 0, s>>>(n, cur, z);
+  MSG_CHECK_LAUNCH();
+  return MSG_OK;
+}
+
 int amg_apply(msg_ctx *c, const double *r, double *z) {
   if (!S(c) || S(c)->lv.empty()) { set_error("AMG hierarchy not built"); return MSG_ERR_STATE; }
+  if (c->prm.precision == 1) return vcycle_mixed(c, r, z);
   return vcycle(c, 0, r, z);
 }
 

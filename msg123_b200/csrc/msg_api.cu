@@ -38,9 +38,18 @@ __global__ void k_scale_copy(int n, double *y, const double *x, double a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = __dmul_rn(x[i], a);
 }
 // outjvec = -(f2 - f1) * eps_inv  (calc_vecjacf, Calc_function.f90:613-617)
+// Newton initial guess: h = h_old + ratio*(h_old - h_old2)
+__global__ void k_extrap(int n, double *h, const double *h_old, const double *h_old2, double ratio) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    h[i] = __dadd_rn(h_old[i], __dmul_rn(ratio, __dsub_rn(h_old[i], h_old2[i])));
+}
 __global__ void k_vecjac_out(int n, double *out, const double *f2, const double *f1, double eps_inv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[i] = __dmul_rn(-__dsub_rn(f2[i], f1[i]), eps_inv);
+}
+__global__ void k_to_f32(size_t n, const double *a, float *b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
 }
 __global__ void k_csr_to_dia(int nx, int ny, int nz, const int *offind, const double *lumat, double *lu) {
   int N = nx * ny * nz, nxy = nx * ny;
@@ -64,9 +73,17 @@ static double sum_part(msg_ctx *c, int count, int *rc) {
 
 // calc_func + its squared norm
 static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
+  if (c->timing) cudaEventRecord(c->ev[7], c->stream);
   int rc = launch_calc_func(c, h, F, true);
   if (rc) return rc;
-  *l2 = sum_part(c, nblk(c->N), &rc);
+  *l2 = sum_part(c, nblk(c->N), &rc);   // synchronises the stream
+  if (c->timing) {
+    cudaEventRecord(c->ev[0], c->stream);
+    cudaEventSynchronize(c->ev[0]);
+    float a = 0.f;
+    cudaEventElapsedTime(&a, c->ev[7], c->ev[0]);
+    c->t_ms[3] += a;
+  }
   return rc;
 }
 
@@ -345,6 +362,7 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
       c->delt_old2 = c->delt_old1; c->delt_old1 = c->delt;
       if (c->prm.sim_type == 0) c->delt = c->delt * c->prm.inc_fact;
       else { apply_heuri(c, last_out); if (c->delt > c->prm.max_step) c->delt = c->prm.max_step; }
+      if ((rc = copy_d2d(c, c->head_old2, c->head_old, n))) return rc;
       if ((rc = copy_d2d(c, c->head_old, c->head_new, n))) return rc;
       if ((rc = copy_d2d(c, c->srat_old, c->srat_new, n))) return rc;
       if ((rc = copy_d2d(c, c->surf_old, c->surf_head, S))) return rc;
@@ -365,8 +383,27 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
     c->current_t = (double)(float)(c->current_t + (double)(float)c->delt);
     c->delt_inv = 1.0 / c->delt;
     msg_stats_t st;
+    bool learned_try = false;
+    if (c->prm.guess_mode == 2 && c->timestep_num > 0 && conv != 0 && learned_ready(c)) {
+      if ((rc = learned_guess(c))) return rc;       // head_new <- h_old + CNN increment
+      learned_try = true;
+    } else if (c->prm.guess_mode >= 1 && c->timestep_num > 0) {
+      k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
+      MSG_CHECK_LAUNCH();
+    }
     rc = calc_numsol(c, &st);
     if (rc < 0) return rc;
+    if (learned_try && rc != MSG_OK) {
+      // fallback: the same time step again from the plain extrapolation
+      R.newton_total += st.out_iter; R.krylov_total += st.inner_total; R.back_total += st.back_total;
+      c->guess_fallbacks++;
+      if ((rc = copy_d2d(c, c->srat_new, c->srat_old, n))) return rc;
+      if ((rc = copy_d2d(c, c->surf_head, c->surf_old, S))) return rc;
+      k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
+      MSG_CHECK_LAUNCH();
+      rc = calc_numsol(c, &st);
+      if (rc < 0) return rc;
+    }
     R.newton_total += st.out_iter; R.krylov_total += st.inner_total; R.back_total += st.back_total;
     last_out = st.out_iter;
     conv = (rc == MSG_OK) ? 1 : 0;
@@ -451,11 +488,15 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
                    &c->drain, &c->surf_head, &c->surf_old};
   for (auto q : sz) { ALLOC(*q, S * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, S * 8, c->stream)); }
   ALLOC(c->offind, (N + 1) * 4);
-  double **vn[] = {&c->head_new, &c->head_old, &c->head_pre, &c->head_change, &c->srat_new, &c->srat_old,
+  double **vn[] = {&c->head_new, &c->head_old, &c->head_old2, &c->head_pre, &c->head_change, &c->srat_new, &c->srat_old,
                    &c->new_f, &c->kr, &c->kr_per, &c->alp, &c->sto, &c->stod, &c->tmpv, &c->dmat, &c->rhs,
                    &c->slope_rhs, &c->dilu_d, &c->r, &c->rs, &c->p, &c->v, &c->t, &c->z};
   for (auto q : vn) { ALLOC(*q, N * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, N * 8, c->stream)); }
   ALLOC(c->lu, 6 * N * 8);
+  if (p->precision == 1) {
+    ALLOC(c->dmat_f, N * 4);
+    ALLOC(c->lu_f, 6 * N * 4);
+  }
   size_t npart = std::max((size_t)kRedBlocks * 8, (size_t)nblk((int)N) + 8);
   ALLOC(c->part, npart * 8);
   MSG_CUDA(cudaMallocHost((void **)&c->hpin, npart * 8));
@@ -510,6 +551,7 @@ int msg_gpu_init_state(msg_ctx_t *c, const double *head, double delt) {
   size_t N = c->N, S = c->S;
   UPLOAD(c->head_new, head, N * 8);
   MSG_CUDA(cudaMemcpyAsync(c->head_old, c->head_new, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  MSG_CUDA(cudaMemcpyAsync(c->head_old2, c->head_new, N * 8, cudaMemcpyDeviceToDevice, c->stream));
   int rc = launch_srat_rperm(c, c->head_new, 0.0, c->srat_old, c->kr, nullptr);
   if (rc) return rc;
   MSG_CUDA(cudaMemcpyAsync(c->srat_new, c->srat_old, N * 8, cudaMemcpyDeviceToDevice, c->stream));
@@ -610,6 +652,12 @@ int msg_gpu_set_system(msg_ctx_t *c, const double *dmat, const double *lumat, co
   UPLOAD(tmp, lumat, (size_t)c->nnz * 8);
   k_csr_to_dia<<<nblk(c->N), kThreads, 0, c->stream>>>(c->nx, c->ny, c->nz, c->offind, tmp, c->lu);
   MSG_CHECK_LAUNCH();
+  if (c->dmat_f) {
+    k_to_f32<<<kRedBlocks, kThreads, 0, c->stream>>>(N, c->dmat, c->dmat_f);
+    MSG_CHECK_LAUNCH();
+    k_to_f32<<<kRedBlocks, kThreads, 0, c->stream>>>(6 * N, c->lu, c->lu_f);
+    MSG_CHECK_LAUNCH();
+  }
   MSG_CUDA(cudaStreamSynchronize(c->stream));
   cudaFree(tmp);
   MSG_CUDA(cudaMemcpyAsync(c->slope_rhs, c->rhs, N * 8, cudaMemcpyDeviceToDevice, c->stream));
@@ -746,13 +794,14 @@ namespace msg {
 static void free_ctx(msg_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   amg_free(c);
+  learned_free(c);
   void *dp[] = {c->reta, c->retn, c->resi, c->poro, c->ss, c->ksz, c->cell_top, c->cell_vol, c->hy, c->ab,
                 c->surf_top, c->surf_bott, c->surf_reli, c->surf_parm, c->hydf_surf, c->abyd_surf, c->calc_rech,
                 c->rech_base, c->sea_hydf, c->sea_abyd, c->read_seal, c->drain, c->offind, c->offrow, c->conn_dir,
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,
                 c->head_change, c->srat_new, c->srat_old, c->surf_head, c->surf_old, c->new_f, c->kr, c->kr_per,
-                c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->slope_rhs, c->dilu_d, c->r, c->rs,
-                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells};
+                c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->head_old2, c->slope_rhs, c->dilu_d, c->r, c->rs,
+                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f};
   for (auto q : dp) if (q) cudaFree(q);
   if (c->hpin) cudaFreeHost(c->hpin);
   for (int k = 0; k < 8; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);

@@ -40,12 +40,13 @@ struct msg_ctx {
   int *offind, *offrow, *conn_dir, *left_off, *right_off;
   double *hydf_conn, *abyd_conn;
   // ---- state -------------------------------------------------------------------------
-  double *head_new, *head_old, *head_pre, *head_change, *srat_new, *srat_old;
+  double *head_new, *head_old, *head_pre, *head_change, *srat_new, *srat_old, *head_old2;
   double *surf_head, *surf_old, *new_f;
   double *kr, *kr_per, *alp, *sto, *stod;        // per-cell vG results / storage terms
   double *tmpv;                                  // [N] spare vector (J.v, line search)
   // ---- level-1 system, DIA: lu[d*N + i] = J(i, nb_d(i)) --------------------------------
   double *dmat, *lu, *rhs, *slope_rhs;
+  float *dmat_f, *lu_f;                          // FP32 images (precision = 1)
   // ---- Krylov work ----------------------------------------------------------------------
   double *dilu_d, *r, *rs, *p, *v, *t, *z;
   msg::DevScalars *sc;                           // device scalars
@@ -64,6 +65,9 @@ struct msg_ctx {
   // ---- time loop ---------------------------------------------------------------------------------
   double current_t, delt_old1, delt_old2;
   int timestep_num, last_conv, last_out;
+  int guess_fallbacks;                           // learned guesses replaced by extrapolation
+  // learned initial guess (msg_learned.cu)
+  void *learned;
   // ---- timing ------------------------------------------------------------------------------------
   cudaEvent_t ev[8];
   double t_ms[5];
@@ -101,6 +105,11 @@ int scale(msg_ctx *c, double *y, double a, int n);
 int amg_setup(msg_ctx *c);
 int amg_apply(msg_ctx *c, const double *r, double *z);
 void amg_free(msg_ctx *c);
+
+// ---- msg_learned.cu ------------------------------------------------------------------------------
+bool learned_ready(msg_ctx *c);
+int learned_guess(msg_ctx *c);
+void learned_free(msg_ctx *c);
 
 // ---- preconditioner dispatch (msg_linear.cu) ---------------------------------------------------------
 int apply_prec(msg_ctx *c, const double *r, double *z);

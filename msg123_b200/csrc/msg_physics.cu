@@ -230,6 +230,7 @@ struct FluxArgs {
   double newper, newper_inv;
   double *F;          // residual (calc_func) or rhs = -F (make_matvec)
   double *dmat, *lu;  // assembly outputs
+  float *dmat_f, *lu_f;   // FP32 images for the mixed-precision V-cycle (nullable)
   double *part;       // partial sums of F^2 (nullable)
 };
 
@@ -308,7 +309,10 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
           dc = __dadd_rn(__dadd_rn(dc, deri_dcon), c1);
         }
       }
-      if (ASM) a.lu[(size_t)d * N + i] = luv;
+      if (ASM) {
+        a.lu[(size_t)d * N + i] = luv;
+        if (a.lu_f) a.lu_f[(size_t)d * N + i] = (float)luv;
+      }
     }
     // boundary terms of the top layer
     double fs = 0.0, ds = 0.0, sea = 0.0, sead = 0.0;
@@ -349,6 +353,7 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
     if (ASM) {
       a.F[i] = -f;
       a.dmat[i] = dd;
+      if (a.dmat_f) a.dmat_f[i] = (float)dd;
     } else {
       a.F[i] = f;
     }
@@ -496,6 +501,7 @@ static FluxArgs flux_args(msg_ctx *c, const double *h) {
   a.drain = c->drain;
   a.newper = c->newper; a.newper_inv = c->newper_inv;
   a.F = nullptr; a.dmat = nullptr; a.lu = nullptr; a.part = nullptr;
+  a.dmat_f = nullptr; a.lu_f = nullptr;
   return a;
 }
 
@@ -526,6 +532,8 @@ int launch_make_matvec(msg_ctx *c) {
   a.F = c->rhs;
   a.dmat = c->dmat;
   a.lu = c->lu;
+  a.dmat_f = c->dmat_f;
+  a.lu_f = c->lu_f;
   a.part = c->part;
   k_flux<true><<<nblk(c->N), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();

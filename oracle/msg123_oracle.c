@@ -56,7 +56,7 @@ typedef struct orc {
   double *surf_area, *rech_area, *hydf_surf, *abyd_surf, *surf_dis;
   double *surf_top, *surf_bott, *surf_reli, *surf_parm;
   double *calc_rech, *rech_base, *drain_coef;
-  double *head_new, *head_old, *head_pre, *head_change, *srat_new, *srat_old;
+  double *head_new, *head_old, *head_pre, *head_change, *srat_new, *srat_old, *head_old2;
   double *rel_perm, *surf_head, *surf_old, *surf_rati, *new_f;
   double *per_srat, *per_relp;
   double delt, delt_inv, newper, newper_inv, len_scal;
@@ -1181,6 +1181,7 @@ static int time_loop(orc_t *o, int nsteps, double rech_until, double rech_after,
       o->delt_old2 = o->delt_old1; o->delt_old1 = o->delt;
       if (o->prm.sim_type == 0) o->delt = o->delt * o->prm.inc_fact;
       else { apply_heuri(o, last_out); if (o->delt > o->prm.max_step) o->delt = o->prm.max_step; }
+      memcpy(o->head_old2, o->head_old, sizeof(double) * n);
       memcpy(o->head_old, o->head_new, sizeof(double) * n);
       memcpy(o->srat_old, o->srat_new, sizeof(double) * n);
       memcpy(o->surf_old, o->surf_head, sizeof(double) * S);
@@ -1200,6 +1201,11 @@ static int time_loop(orc_t *o, int nsteps, double rech_until, double rech_after,
     for (int s = 0; s < S; ++s) o->calc_rech[s] = o->rech_base[s] * scale;
     o->current_t = (double)(float)(o->current_t + (double)(float)o->delt);
     o->delt_inv = DONE / o->delt;
+    /* Newton initial guess (extension): linear extrapolation in time */
+    if (o->prm.guess_mode == 1 && o->timestep_num > 0) {
+      double ratio = o->delt / o->delt_old1;
+      for (int i = 0; i < n; ++i) o->head_new[i] = o->head_old[i] + ratio * (o->head_old[i] - o->head_old2[i]);
+    }
     msg_stats_t st;
     int rc = calc_numsol(o, &st);
     R.newton_total += st.out_iter; R.krylov_total += st.inner_total; R.back_total += st.back_total;
@@ -1274,6 +1280,7 @@ void *orc_create(const msg_grid_t *g, const msg_params_t *p) {
   o->read_seal = dupd(g->sea_head, S);
   orc_connect(o);
   o->head_new = xc(N, 8); o->head_old = xc(N, 8); o->head_pre = xc(N, 8); o->head_change = xc(N, 8);
+  o->head_old2 = xc(N, 8);
   o->srat_new = xc(N, 8); o->srat_old = xc(N, 8); o->rel_perm = xc(N, 8); o->new_f = xc(N, 8);
   o->per_srat = xc(N, 8); o->per_relp = xc(N, 8); o->slope_rhs = xc(N, 8);
   o->surf_head = xc(S, 8); o->surf_old = xc(S, 8); o->surf_rati = xc(S, 8);
@@ -1299,7 +1306,7 @@ void orc_destroy(void *h) {
                   o->surf_area, o->rech_area, o->hydf_surf, o->abyd_surf, o->surf_dis, o->surf_top, o->surf_bott,
                   o->surf_reli, o->surf_parm, o->calc_rech, o->rech_base, o->drain_coef, o->head_new, o->head_old,
                   o->head_pre, o->head_change, o->srat_new, o->srat_old, o->rel_perm, o->surf_head, o->surf_old,
-                  o->surf_rati, o->new_f, o->per_srat, o->per_relp, o->slope_rhs};
+                  o->surf_rati, o->new_f, o->per_srat, o->per_relp, o->slope_rhs, o->head_old2};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   free(o);
 }
@@ -1333,7 +1340,7 @@ void orc_set_state(void *h, const double *head_new, const double *head_old, cons
  * the initial head, srat from calc_srat_rperm, surface heads from the head. */
 void orc_init_state(void *h, const double *head, double delt) {
   orc_t *o = h; int N = o->ncalc, S = o->ncals;
-  memcpy(o->head_new, head, 8 * N); memcpy(o->head_old, head, 8 * N);
+  memcpy(o->head_new, head, 8 * N); memcpy(o->head_old, head, 8 * N); memcpy(o->head_old2, head, 8 * N);
   srat_rperm(o, DZERO, head, o->srat_old, o->rel_perm, NULL);
   memcpy(o->srat_new, o->srat_old, 8 * N);
   memcpy(o->surf_head, head, 8 * S); memcpy(o->surf_old, head, 8 * S);
