@@ -87,7 +87,8 @@ typedef struct msg_params {
   double end_time;           /* simulation end (s)                                                    */
   int32_t guess_mode;        /* Newton initial guess: 0 = previous head (reference), 1 = linear
                                 extrapolation, 2 = learned increment (extrapolation on failure)      */
-  int32_t pad2;
+  int32_t guess_select;      /* guess_mode 2: 1 = start from whichever of the learned and the
+                                extrapolated guess has the smaller ||F|| (two residual evaluations) */
 } msg_params_t;
 
 /* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */
@@ -224,6 +225,37 @@ MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv);
  * the first call on a device looks up its address and should precede any stream
  * capture; concurrent calls on one device race on that workspace. */
 MSG_API int msg_gpu_dense_inverse_noalloc(int32_t n, const double *a_dev, double *inv_dev, void *stream);
+
+/* ---- learned Newton initial guess (no counterpart in the reference) ----------------------
+ * A 3D CNN (four 3x3x3 convolutions, 16 channels, GELU, BF16 weights and activations,
+ * FP32 accumulation on the tensor cores) predicts the correction to the linear
+ * extrapolation of the head: h0 = h_t + r (h_t - h_{t-1}) + s * CNN(features).
+ * Used by calc_numsol's time loop when guess_mode = 2; a step whose Newton solve fails
+ * from the learned guess is retried from the plain extrapolation. */
+typedef struct msg_cnn msg_cnn_t;
+MSG_API int msg_gpu_cnn_create(int32_t seed, msg_cnn_t **out);
+MSG_API void msg_gpu_cnn_destroy(msg_cnn_t *cnn);
+MSG_API int msg_gpu_cnn_nparam(void);
+/* corrections whose normalised size |o| is at most `dead` are dropped (default 0.1) */
+MSG_API int msg_gpu_cnn_set_deadband(msg_cnn_t *cnn, float dead);
+MSG_API int msg_gpu_cnn_get_weights(msg_cnn_t *cnn, float *w);
+MSG_API int msg_gpu_cnn_set_weights(msg_cnn_t *cnn, const float *w);
+/* append a training sample from a context right after an accepted step */
+MSG_API int msg_gpu_cnn_collect(msg_cnn_t *cnn, msg_ctx_t *ctx);
+MSG_API int msg_gpu_cnn_nsamples(msg_cnn_t *cnn);
+/* append a sample from host arrays: x [N][16] features, y [N] target, N = nx*ny*nz */
+MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *cnn, int32_t nx, int32_t ny, int32_t nz, const float *x, const float *y);
+/* mean squared error on one sample; grad (msg_gpu_cnn_nparam floats) and out (N) may be NULL */
+MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *cnn, int32_t sample, double *loss, float *grad, float *out);
+/* AdamW training over the stored samples */
+MSG_API int msg_gpu_cnn_train(msg_cnn_t *cnn, int32_t iters, float lr, float weight_decay, int32_t seed,
+                              double *mean_loss);
+/* use the network in a context (guess_mode = 2); NULL detaches */
+MSG_API int msg_gpu_cnn_attach(msg_ctx_t *ctx, msg_cnn_t *cnn);
+/* learned guesses replaced by the extrapolation after a failed Newton solve */
+MSG_API int msg_gpu_guess_fallbacks(msg_ctx_t *ctx);
+/* learned guesses not used because the extrapolation had the smaller residual */
+MSG_API int msg_gpu_guess_rejected(msg_ctx_t *ctx);
 
 /* Number of kernels this library has launched in this process (all contexts). */
 MSG_API long long msg_gpu_launch_count(void);

@@ -51,7 +51,7 @@ class MsgParams(C.Structure):
         ("jac_omega", C.c_float), ("amg_theta", C.c_float), ("smooth_omega", C.c_float),
         ("sim_type", C.c_int32), ("amg_lag", C.c_int32),
         ("ini_step", C.c_double), ("inc_fact", C.c_double), ("max_step", C.c_double),
-        ("end_time", C.c_double), ("guess_mode", C.c_int32), ("pad2", C.c_int32),
+        ("end_time", C.c_double), ("guess_mode", C.c_int32), ("guess_select", C.c_int32),
     ]
 
 

@@ -387,6 +387,19 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
     if (c->prm.guess_mode == 2 && c->timestep_num > 0 && conv != 0 && learned_ready(c)) {
       if ((rc = learned_guess(c))) return rc;       // head_new <- h_old + CNN increment
       learned_try = true;
+      if (c->prm.guess_select) {
+        // keep the learned guess only if its residual is below the extrapolation's
+        double fl = 0.0, fe = 0.0;
+        if ((rc = func_norm(c, c->head_new, c->new_f, &fl))) return rc;
+        k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_pre, c->head_old, c->head_old2, c->delt / c->delt_old1);
+        MSG_CHECK_LAUNCH();
+        if ((rc = func_norm(c, c->head_pre, c->new_f, &fe))) return rc;
+        if (!(fl < fe)) {
+          if ((rc = copy_d2d(c, c->head_new, c->head_pre, n))) return rc;
+          learned_try = false;
+          c->guess_rejected++;
+        }
+      }
     } else if (c->prm.guess_mode >= 1 && c->timestep_num > 0) {
       k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
       MSG_CHECK_LAUNCH();

@@ -66,6 +66,7 @@ struct msg_ctx {
   double current_t, delt_old1, delt_old2;
   int timestep_num, last_conv, last_out;
   int guess_fallbacks;                           // learned guesses replaced by extrapolation
+  int guess_rejected;                            // learned guesses not used (larger residual)
   // learned initial guess (msg_learned.cu)
   void *learned;
   // ---- timing ------------------------------------------------------------------------------------
