@@ -1,20 +1,26 @@
 """Benchmark: simulated cell-timesteps per second of the Newton-Krylov Richards solver.
 
-One "step" is one accepted implicit time step (calc_numsol: Jacobian assembly,
-AMG/ILU setup, BiCGStab, line search) over the whole grid.  value = cells x
-accepted steps / device time of the K timed steps (CUDA events on the library's
-stream).  e2e = the same metric through the public C ABI with the state in host
-memory: every step copies head_new / head_old / srat_old / surf_head in and
-head_new / srat_new out (the way a Fortran caller of calc_numsol holds its state).
+One step is one accepted implicit time step (calc_numsol: Jacobian assembly, AMG
+setup, BiCGStab, line search) over the whole grid.  The workload is the
+512x512x96 heterogeneous block (25,165,824 cells, sigma_lnK = 1.5, rain 20 mm/h,
+adaptive steps from 600 s, Newton tolerance 1e-8 relative head), synthetic and seeded.
 
-Workloads (synthetic, seeded; see msg123_b200/config.py):
-  hetero : 256x256x64 heterogeneous block, plain FP64 BiCGStab + AMG (default)
-  box    : 20x20x50 infiltration box, BiCGStab + ILU(0)
-  large  : 512x512x96 block
+* value     : mixed precision + learned initial guess (FP32/BF16 V-cycle, FP64 Krylov and
+              Newton, AMG hierarchy kept per time step, CNN guess with extrapolation
+              fallback); cells x accepted steps / device time of the K timed steps
+              (CUDA events on the library stream).
+* plain_fp64: the reference's method on the same field on the GPU (FP64 everywhere,
+              AMG rebuilt at every Newton iteration, Newton started from the previous
+              head), the path the north-star ratio is taken against.
+* e2e       : the mixed+learned path through the public C ABI with the state in host
+              memory (head/srat/surface copied in and out through set_state/get_state
+              every step).
+* cpu_baseline / --impl reference: the C restatement of the reference path (OpenMP,
+              all host cores) on a bounded block of the same generator.
 
 Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Multi-GPU (torchrun): every rank solves its own seeded realisation; no data-path
-collective exists (independent replicas), value = sum of cells x steps / max time.
+Multi-GPU (torchrun): every rank solves its own seeded realisation (independent
+replicas, no data-path collective); value = sum of cells x steps / max time.
 """
 import argparse
 import json
@@ -29,25 +35,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+METRIC = "cell-timesteps/s at 1e-8 rel head tol"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
-# Algorithmic bytes per cell for the kernel classes timed by msg_gpu_kernel_time
-# (compulsory traffic, neighbour reads assumed cache-reused):
-#  SpMV FP64 DIA: d 8 + six off-diagonals 48 + x 8 + y 8
-#  calc_func    : vG pass (h 8, top 8, 5 params 20, h_old 8, S_old 8, vol 8 -> S 8, kr 8, sto 8)
-#                 + flux pass (h 8, kr 8, hy 24, ab 24, sto 8 -> F 8)
-#  make_matvec  : vG pair pass (inputs 60 -> S, kr, kr_per, sto, stod 40)
-#                 + assembly pass (h, kr, kr_per 24, hy, ab 48, sto, stod 16 -> rhs, dmat 16, lu 48)
-ALG_BYTES = {0: 72.0, 1: 84.0 + 80.0, 2: 100.0 + 152.0}
-KERNEL_NAMES = {0: "stencil SpMV (FP64, DIA)", 1: "calc_func (vG + flux)", 2: "make_matvec (vG pair + assembly)"}
+# Algorithmic bytes per cell of the kernels timed by msg_gpu_kernel_time (compulsory
+# HBM traffic, neighbour reads cache-reused):
+#  0 SpMV FP64 DIA : d 8 + six off-diagonals 48 + x 8 + y 8
+#  1 calc_func     : vG pass (h, top, 5 params 20, h_old, S_old, vol -> S, kr, sto) 84
+#                    + flux pass (h, kr, hy 24, ab 24, sto -> F) 80
+#  2 make_matvec   : vG pair pass (h, top, params 20, h_old, S_old, vol -> S, kr, kr_per,
+#                    sto, stod) 100 + assembly pass (h, kr, kr_per, hy, ab, sto, stod ->
+#                    rhs, dmat, six lu, FP32 images 28) 180
+ALG_BYTES = {0: 72.0, 1: 164.0, 2: 280.0}
+KERNEL_NAMES = {0: "stencil SpMV (FP64, DIA)", 1: "calc_func (vG + flux)",
+                2: "make_matvec (vG pair + Jacobian assembly)"}
 
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
-            d = json.load(f)
-        return d, "measured"
+            return json.load(f), "measured"
     return PEAKS_FALLBACK, "fallback"
 
 
@@ -88,28 +96,14 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        num = lambda v: v.replace(".", "", 1).isdigit()
+        sm = [float(s[0]) for s in self.samples if num(s[0])]
+        mx = [float(s[1]) for s in self.samples if num(s[1])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and
-                          s[3 + k].lower() == "active"})
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and s[3 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
-
-
-def make_problem(args, rank):
-    from msg123_b200.config import make_config
-    kw = {}
-    if args.shape:
-        kw["shape"] = tuple(int(v) for v in args.shape.split("x"))
-    if args.workload in ("hetero", "large"):
-        kw["seed"] = 2024 + rank
-    p = make_config(args.workload, **kw)
-    if args.precision == "mixed":
-        p.params["precision"] = 1
-    if args.precon:
-        p.params["precon_type"] = 0 if args.precon == "ilu" else 1
-    return p
 
 
 def dist_setup():
@@ -131,88 +125,86 @@ def barrier(dist):
         dist.barrier()
 
 
-def allmax(dist, v):
+def reduce(dist, v, op):
     if dist is None:
         return v
     import torch
     t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
 
-def allsum(dist, v):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+def make_problem(args, rank):
+    from msg123_b200.config import make_config
+    kw = {"seed": 2024 + rank}
+    if args.shape:
+        kw["shape"] = tuple(int(v) for v in args.shape.split("x"))
+    return make_config(args.workload, **kw)
 
 
-def cpu_baseline(args, prob, budget_s=20.0):
-    """The oracle (C restatement, OpenMP) on a bounded prefix of the same workload."""
+FAST = dict(precision=1, amg_lag=1, guess_mode=2, guess_select=1)
+PLAIN = dict(precision=0, amg_lag=0, guess_mode=0)
+
+
+def workload_config(args, prob):
+    prm = prob.params
+    return {"workload": f"{args.workload} {prob.nx}x{prob.ny}x{prob.nz} ({prob.ncalc} cells), heterogeneous "
+                        f"lnKs field, 20 mm/h rain, adaptive dt from {prm['ini_step']:.0f} s",
+            "solver": "Newton (Eisenstat-Walker, cubic line search) + BiCGStab + smoothed-aggregation AMG",
+            "value_path": "mixed precision (FP32 V-cycle, BF16 coarse operators, FP64 Krylov/Newton/coarse LU) + "
+                          "learned initial guess (extrapolation fallback), AMG hierarchy per time step",
+            "baseline_path": "plain FP64, AMG rebuilt every Newton iteration, Newton from the previous head",
+            "newton_tol": "max|dh| <= 1e-8 max|h|",
+            "l2": "inputs larger than L2 (126 MB); no flush needed",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def timed_advance(g, steps):
+    rc, st = g.advance(nsteps=steps)
+    return st, g.timers()["total_ms"]
+
+
+def cpu_run(prob, budget_s, max_steps):
+    """Oracle (C restatement, OpenMP) on the plain FP64 path, bounded in time."""
     from oracle.oracle import Oracle
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    o = Oracle(prob)
+    o = Oracle(prob, **PLAIN)
     o.init_state()
-    steps = 0
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < budget_s and steps < max(1, args.steps):
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and steps < max_steps:
         rc, st = o.advance(nsteps=1)
         if rc != 0:
             break
         steps += 1
     dt = time.perf_counter() - t0
     o.close()
-    return {"value": prob.ncalc * steps / dt, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
-            "sample": f"first {steps} accepted step(s) of the same {prob.nx}x{prob.ny}x{prob.nz} workload, "
-                      f"C restatement (oracle/msg123_oracle.c, -O2, OpenMP) in {dt:.1f} s"}
+    return prob.ncalc * max(steps, 1) / dt, steps, dt, threads
+
+
+def cpu_sample_problem(args):
+    from msg123_b200.config import make_config
+    return make_config(args.workload, shape=tuple(int(v) for v in args.cpu_shape.split("x")), seed=2024)
 
 
 def run_reference(args):
     rank, ws, dist = dist_setup()
-    if rank != 0:
-        return
-    prob = make_problem(args, 0)
-    from oracle.oracle import Oracle
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    o = Oracle(prob)
-    o.init_state()
-    for _ in range(args.warmup):
-        o.advance(nsteps=1)
-        break   # one warm-up step bounds the CPU time; later warm-ups repeat the same work
-    t0 = time.perf_counter()
-    steps = 0
-    budget = 120.0
-    while steps < args.steps and time.perf_counter() - t0 < budget:
-        rc, st = o.advance(nsteps=1)
-        steps += 1
-    dt = time.perf_counter() - t0
-    val = prob.ncalc * steps / dt
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "cell-timesteps/s", "n_gpus": ws,
-            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(steps, 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, prob),
-            "cpu_baseline": {"value": val, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
-                             "sample": f"{steps} step(s) of the workload (bounded to {budget:.0f} s)"},
-            "e2e": {"value": val, "unit": "cell-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
-
-
-METRIC = "cell-timesteps/s"
-
-
-def workload_config(args, prob):
-    prm = prob.params
-    prec = {0: "ILU(0)/DILU", 1: "AMG"}[prm["precon_type"]]
-    return {"workload": f"{prob.name} {prob.nx}x{prob.ny}x{prob.nz} ({prob.ncalc} cells)",
-            "solver": f"Newton + BiCGStab + {prec}" + (" (reference quirks)" if prm["ref_quirks"] else ""),
-            "precision": "fp64" if prm["precision"] == 0 else "mixed (fp32 V-cycle, bf16 coarse)",
-            "newton_tol": f"{prm['criteria']} x max|h| (relative)" if prm["criteria_rel"] else prm["criteria"],
-            "l2": "inputs larger than L2 (126 MB)" if prob.ncalc * 8 * 20 > 126e6 else "small case, L2 resident",
-            "parallelism": f"replicas x{args.gpus}"}
+    if rank == 0:
+        prob = cpu_sample_problem(args)
+        val, steps, dt, threads = cpu_run(prob, budget_s=60.0, max_steps=max(1, args.steps))
+        sample = (f"{steps} accepted step(s) of a {prob.nx}x{prob.ny}x{prob.nz} block of the same generator "
+                  f"(plain FP64 path), C restatement oracle/msg123_oracle.c with OpenMP, {dt:.1f} s")
+        line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "cell-timesteps/s", "n_gpus": ws,
+                "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / max(steps, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"{args.workload} generator, {prob.nx}x{prob.ny}x{prob.nz} block",
+                           "path": "plain FP64 (reference method)"},
+                "cpu_baseline": {"value": val, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": val, "unit": "cell-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def main():
@@ -221,12 +213,13 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hetero", choices=["hetero", "box", "large"])
+    ap.add_argument("--workload", default="large", choices=["large", "hetero", "box"])
     ap.add_argument("--shape", default="")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--precon", default="", choices=["", "ilu", "amg"])
+    ap.add_argument("--cpu-shape", default="96x96x96")
+    ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -236,34 +229,34 @@ def main():
     if rank == 0 and build.needs_build():
         build.build()
     barrier(dist)
+    from msg123_b200.learned import Cnn
     from msg123_b200.solver import GpuSolver, launch_count
+    from msg123_b200.train_guess import load
     prob = make_problem(args, rank)
-    g = GpuSolver(prob)
+    cnn = load(Cnn(seed=0))
+
+    # ---- mixed precision + learned guess: the headline -------------------------------
+    g = GpuSolver(prob, **FAST)
+    cnn.attach(g)
     g.init_state()
-    # warm-up steps (untimed)
-    rc, st_w = g.advance(nsteps=args.warmup)
+    g.advance(nsteps=args.warmup)
     barrier(dist)
     l0 = launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        rc, st = g.advance(nsteps=args.steps)
+        st, ms = timed_advance(g, args.steps)
     launches = launch_count() - l0
-    ms = g.timers()["total_ms"]
-    tmax = allmax(dist, ms)
-    cells_steps = allsum(dist, float(prob.ncalc * st["accepted"]))
-    value = cells_steps / (tmax * 1e-3)
+    tmax = reduce(dist, ms, "max")
+    value = reduce(dist, float(prob.ncalc * st["accepted"]), "sum") / (tmax * 1e-3)
 
-    # kernel timings for the roofline (same context, state of the last timed step)
+    # kernel timings for the roofline (state of the last timed step, library stream)
     peaks, src = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
-    kt = {}
-    for which in (0, 1, 2):
-        t = g.kernel_time(which, reps=10)
-        kt[which] = t
-    dom = 2   # the assembly pass is timed as the dominant bandwidth kernel
-    achieved = ALG_BYTES[dom] * prob.ncalc / (kt[dom] * 1e-3) / 1e9
-    spmv_gbs = ALG_BYTES[0] * prob.ncalc / (kt[0] * 1e-3) / 1e9
+    kt = {w: g.kernel_time(w, reps=10) for w in (0, 1, 2)}
+    gbs = {w: ALG_BYTES[w] * prob.ncalc / (kt[w] * 1e-3) / 1e9 for w in kt}
+    t_prec = g.kernel_time(3, reps=5)
+    t_setup = g.kernel_time(4, reps=2)
 
-    # end-to-end through the public API with host-resident state
+    # end to end through the public API, state in host memory
     e2e = None
     if not args.no_e2e:
         s = g.get_state()
@@ -276,37 +269,61 @@ def main():
             g.set_state(head_new=h_new, head_old=h_old, srat_old=s_old, surf_head=surf)
             rc2, st2 = g.advance(nsteps=1)
             s2 = g.get_state()
-            h_old, s_old, surf = s2["head_new"], s2["srat_new"], s2["surf_head"]
-            h_new = h_old
+            h_new, h_old, s_old, surf = s2["head_new"], s2["head_old"], s2["srat_new"], s2["surf_head"]
             acc += st2["accepted"]
-        te = time.perf_counter() - t0
-        te = allmax(dist, te)
-        e2e = {"value": allsum(dist, float(prob.ncalc * acc)) / te, "unit": "cell-timesteps/s",
+        te = reduce(dist, time.perf_counter() - t0, "max")
+        e2e = {"value": reduce(dist, float(prob.ncalc * acc), "sum") / te, "unit": "cell-timesteps/s",
                "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 5 * N * 8 + S * 8,
-               "note": "state copied in and out through msg_gpu_set_state / msg_gpu_get_state every step"}
+               "path": "mixed + learned through msg_gpu_set_state / msg_gpu_advance / msg_gpu_get_state"}
+    g.close()
+
+    # ---- plain FP64 reference method on the same field ----------------------------------
+    plain = None
+    if not args.no_plain:
+        gp = GpuSolver(prob, **PLAIN)
+        gp.init_state()
+        gp.advance(nsteps=1)
+        barrier(dist)
+        stp, msp = timed_advance(gp, args.plain_steps)
+        tpm = reduce(dist, msp, "max")
+        pv = reduce(dist, float(prob.ncalc * stp["accepted"]), "sum") / (tpm * 1e-3)
+        plain = {"value": pv, "ms_per_step": tpm / max(stp["accepted"], 1),
+                 "newton_per_step": stp["newton_total"] / max(stp["accepted"], 1),
+                 "krylov_per_step": stp["krylov_total"] / max(stp["accepted"], 1),
+                 "steps": stp["accepted"], "simulated_s_per_step": None,
+                 "speedup_of_value": value / pv}
+        gp.close()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args, make_problem(args, 0))
+        cp = cpu_sample_problem(args)
+        val, steps, dt, threads = cpu_run(cp, budget_s=25.0, max_steps=args.steps)
+        cpu = {"value": val, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
+               "sample": f"{steps} accepted step(s) of a {cp.nx}x{cp.ny}x{cp.nz} block of the same generator on the "
+                         f"plain FP64 path, C restatement oracle/msg123_oracle.c with OpenMP ({dt:.1f} s)"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-timesteps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tmax / max(st["accepted"], 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prob.params["precision"] == 0 else "f64+f32",
-            "data": "synthetic", "config": workload_config(args, prob),
-            "newton": {"accepted": st["accepted"], "rejected": st["rejected"], "newton_total": st["newton_total"],
-                       "krylov_total": st["krylov_total"], "backtracks": st["back_total"],
-                       "simulated_s": st["current_t"]},
-            "roofline": {"kernel": KERNEL_NAMES[dom], "bound": "hbm", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
-                         "alg_bytes_per_cell": ALG_BYTES[dom], "ms_per_launch": kt[dom], "traffic": None,
-                         "spmv_gbs": spmv_gbs, "spmv_frac": spmv_gbs / hbm,
-                         "kernel_ms": {KERNEL_NAMES[k]: v for k, v in kt.items()}},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (Krylov/Newton) + f32/bf16 (V-cycle)",
+            "data": "synthetic (seeded lnKs field and van Genuchten draws)", "config": workload_config(args, prob),
+            "newton": {"accepted": st["accepted"], "rejected": st["rejected"],
+                       "newton_per_step": st["newton_total"] / max(st["accepted"], 1),
+                       "krylov_per_step": st["krylov_total"] / max(st["accepted"], 1),
+                       "backtracks": st["back_total"], "simulated_s": st["current_t"]},
+            "plain_fp64": plain,
+            "roofline": {"kernel": KERNEL_NAMES[2], "bound": "hbm", "achieved": gbs[2], "peak": hbm,
+                         "unit": "GB/s", "frac": gbs[2] / hbm, "peak_source": src,
+                         "alg_bytes_per_cell": ALG_BYTES[2], "cells_per_launch": prob.ncalc,
+                         "ms_per_launch": kt[2], "traffic": None,
+                         "others": {KERNEL_NAMES[w]: {"ms": kt[w], "GB/s": gbs[w], "frac": gbs[w] / hbm}
+                                    for w in (0, 1)},
+                         "vcycle_mixed_ms": t_prec, "amg_setup_ms": t_setup},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }
-        print(json.dumps(line))
-    g.close()
+        print(json.dumps(line), flush=True)
+    cnn.close()
     if dist is not None:
         dist.destroy_process_group()
 
