@@ -80,7 +80,8 @@ typedef struct msg_params {
   float amg_theta;           /* strength threshold (real(SP))                                          */
   float smooth_omega;        /* Jacobi smoother weight                                                */
   int32_t sim_type;          /* 0: delt*inc_fact per accepted step; 1: heuristic (apply_heuri)         */
-  int32_t amg_lag;           /* 0: AMG rebuilt at every make_matvec (reference); 1: once per time step */
+  int32_t amg_lag;           /* 0: AMG rebuilt at every make_matvec (reference); k >= 1: rebuilt at the
+                                first Newton iteration of every k-th time step                         */
   double ini_step;           /* initial delt (s)                                                      */
   double inc_fact;           /* factor for sim_type 0                                                 */
   double max_step;           /* cap on delt for sim_type 1                                            */

@@ -1052,7 +1052,7 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
   cudaStream_t s = c->stream;
   const int n = L.n, sw = std::max(c->prm.amg_sweeps, 0);
   const double w = (double)c->prm.smooth_omega;
-  const int g = std::min(nb(n), kRedBlocks * 4);
+  const int g = nb(n);
   const bool last = (l == (int)A->lv.size() - 1);
   if (last && L.cinv) {
     k_gemv<<<nb(n), kThreads, 0, s>>>(n, L.cinv, b, x);
@@ -1110,7 +1110,7 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
   cudaStream_t s = c->stream;
   const int n = L.n, sw = std::max(c->prm.amg_sweeps, 0);
   const float w = c->prm.smooth_omega;
-  const int g = std::min(nb(n), kRedBlocks * 4);
+  const int g = nb(n);
   const bool last = (l == (int)A->lv.size() - 1);
   if (last && L.cinv) {
     k_gemv_mixed<<<nb(n), kThreads, 0, s>>>(n, L.cinv, b, x);
@@ -1156,7 +1156,7 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   cudaStream_t s = c->stream;
   const int n = c->N, sw = std::max(c->prm.amg_sweeps, 0);
   const float w = c->prm.smooth_omega;
-  const int g = std::min(nb(n), kRedBlocks * 4);
+  const int g = nb(n);
   Dia32 D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, c->lu_f};
   const bool single = (A->lv.size() == 1);
   float *cur = A->x0f, *oth = A->t0f;

@@ -62,13 +62,9 @@ __global__ void k_csr_to_dia(int nx, int ny, int nz, const int *offind, const do
 }
 
 static double sum_part(msg_ctx *c, int count, int *rc) {
-  *rc = MSG_OK;
-  cudaError_t e = cudaMemcpyAsync(c->hpin, c->part, (size_t)count * 8, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) { set_error("partials: %s", cudaGetErrorString(e)); *rc = MSG_ERR_CUDA; return 0.0; }
-  double s = 0.0;
-  for (int b = 0; b < count; ++b) s += c->hpin[b];
-  return s;
+  double v = 0.0;
+  *rc = finish(c, count, 1, &v);
+  return v;
 }
 
 // calc_func + its squared norm
@@ -98,9 +94,14 @@ static int make_matvec(msg_ctx *c, double *l2_rhs) {
   if (l2_rhs) *l2_rhs = s;
   if (c->timing) cudaEventRecord(ev[1], c->stream);
   if (c->prm.precon_type == 1 && !c->prm.ref_quirks) {
-    // amg_lag = 1 keeps the hierarchy of the time step's first Newton iteration
-    if (!c->prm.amg_lag || c->out_iter <= 1 || c->amg_nlevel <= 1)
+    // amg_lag = k >= 1: the hierarchy built at a time step's first Newton iteration is
+    // kept for that step and the next k-1 steps (the level-1 smoother always uses the
+    // current Jacobian)
+    if (!c->prm.amg_lag || c->amg_nlevel <= 1 || c->amg_force || (c->out_iter <= 1 && c->amg_age >= c->prm.amg_lag)) {
       if ((rc = amg_setup(c))) return rc;
+      c->amg_age = 0;
+      c->amg_force = 0;
+    }
   }
   if (c->timing) {
     cudaEventRecord(ev[2], c->stream);
@@ -145,7 +146,7 @@ static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out) {
   double eps_inv = 1.0 / eps;
   if ((rc = axpby(c, jc, x, eps, v, n))) return rc;
   if ((rc = func_norm(c, jc, f2, &dummy))) return rc;
-  k_vecjac_out<<<kRedBlocks, 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
+  k_vecjac_out<<<nblk(n), 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -281,6 +282,7 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
   msg_stats_t st;
   memset(&st, 0, sizeof(st));
   double l2x;
+  c->amg_age++;
   if ((rc = dot(c, c->head_new, c->head_new, n, &l2x))) return rc;      // set_backtr
   c->maxstep = std::sqrt(l2x) * VARMAX;
   if (c->maxstep < 1.0) c->maxstep = 1.0;
@@ -391,7 +393,7 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
         // keep the learned guess only if its residual is below the extrapolation's
         double fl = 0.0, fe = 0.0;
         if ((rc = func_norm(c, c->head_new, c->new_f, &fl))) return rc;
-        k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_pre, c->head_old, c->head_old2, c->delt / c->delt_old1);
+        k_extrap<<<nblk(n), 256, 0, c->stream>>>(n, c->head_pre, c->head_old, c->head_old2, c->delt / c->delt_old1);
         MSG_CHECK_LAUNCH();
         if ((rc = func_norm(c, c->head_pre, c->new_f, &fe))) return rc;
         if (!(fl < fe)) {
@@ -401,7 +403,7 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
         }
       }
     } else if (c->prm.guess_mode >= 1 && c->timestep_num > 0) {
-      k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
+      k_extrap<<<nblk(n), 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
       MSG_CHECK_LAUNCH();
     }
     rc = calc_numsol(c, &st);
@@ -412,7 +414,7 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
       c->guess_fallbacks++;
       if ((rc = copy_d2d(c, c->srat_new, c->srat_old, n))) return rc;
       if ((rc = copy_d2d(c, c->surf_head, c->surf_old, S))) return rc;
-      k_extrap<<<kRedBlocks, 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
+      k_extrap<<<nblk(n), 256, 0, c->stream>>>(n, c->head_new, c->head_old, c->head_old2, c->delt / c->delt_old1);
       MSG_CHECK_LAUNCH();
       rc = calc_numsol(c, &st);
       if (rc < 0) return rc;
@@ -510,9 +512,10 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
     ALLOC(c->dmat_f, N * 4);
     ALLOC(c->lu_f, 6 * N * 4);
   }
-  size_t npart = std::max((size_t)kRedBlocks * 8, (size_t)nblk((int)N) + 8);
+  size_t npart = std::max((size_t)kRedBlocks * 8, 2 * (size_t)nblk((int)N) + 64);
   ALLOC(c->part, npart * 8);
-  MSG_CUDA(cudaMallocHost((void **)&c->hpin, npart * 8));
+  ALLOC(c->dres, 16 * 8);
+  MSG_CUDA(cudaMallocHost((void **)&c->hpin, (size_t)kRedBlocks * 8 * 8));
   int rc = build_connectivity(c, g);
   if (rc) return rc;
   if (p->precon_type == 0 || p->ref_quirks) {
@@ -636,7 +639,7 @@ int msg_gpu_calc_func(msg_ctx_t *c, const double *infx, double *funcv) {
 
 int msg_gpu_make_matvec(msg_ctx_t *c, double *dmat, double *lumat, double *rhs) {
   if (!c) return MSG_ERR_ARG;
-  c->out_iter = 0;   // a direct call always rebuilds the hierarchy
+  c->amg_force = 1;   // a direct call always rebuilds the hierarchy
   double l2;
   int rc = make_matvec(c, &l2);
   if (rc) return rc;
@@ -814,7 +817,7 @@ static void free_ctx(msg_ctx *c) {
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,
                 c->head_change, c->srat_new, c->srat_old, c->surf_head, c->surf_old, c->new_f, c->kr, c->kr_per,
                 c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->head_old2, c->slope_rhs, c->dilu_d, c->r, c->rs,
-                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f};
+                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f, c->dres};
   for (auto q : dp) if (q) cudaFree(q);
   if (c->hpin) cudaFreeHost(c->hpin);
   for (int k = 0; k < 8; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);

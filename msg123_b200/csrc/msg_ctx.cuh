@@ -52,13 +52,14 @@ struct msg_ctx {
   msg::DevScalars *sc;                           // device scalars
   msg::DevScalars *sc_host;                      // pinned mirror
   double *part;                                  // reduction partials [kRedBlocks * 8]
-  double *hpin;                                  // pinned host scalars [64]
+  double *hpin;                                  // pinned host scalars
+  double *dres;                                  // device reduction results [16]
   // ---- wavefront ordering for DILU --------------------------------------------------------
   int *plane_ptr, *plane_cells;
   int nplanes;
   // ---- AMG ----------------------------------------------------------------------------------
   void *amg;                                     // msg::AmgState (msg_amg.cu)
-  int amg_nlevel;
+  int amg_nlevel, amg_age, amg_force;
   // ---- Newton module variables (Nonlinear_solution.f90:24-27) ---------------------------------
   int back_iter, back_flag, beta_iter, in_iter, conv_flag, out_iter;
   double maxvar, l2_new, l2_pre, l2_jnorm, lam, eta, gradient, maxstep, errtol, bnorm, rnorm;
@@ -96,6 +97,8 @@ int launch_spmv(msg_ctx *c, const double *x, double *y);
 int solve_bicgs(msg_ctx *c, double *x);      // x in/out (device), uses c->rhs, c->bnorm, c->errtol
 // reductions (results land in c->hpin after a sync)
 int dot(msg_ctx *c, const double *a, const double *b, int n, double *out);   // sync + host value
+// sum narr partial arrays (nparts each, consecutive in c->part) on the device; sync; host values
+int finish(msg_ctx *c, int nparts, int narr, double *out);
 int norm1(msg_ctx *c, const double *a, int n, double *out);
 int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan);
 int lam_length(msg_ctx *c, const double *dh, const double *hn, double *out);

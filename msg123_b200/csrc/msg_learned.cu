@@ -422,11 +422,8 @@ static int cnn_pack(Net &n) {
 static double host_sumsq_diff(msg_ctx *c, const double *a, const double *b, int *rc) {
   const int B = kRedBlocks;
   k_sumsq_diff<<<B, 256, 0, c->stream>>>(c->N, a, b, c->part);
-  cudaMemcpyAsync(c->hpin, c->part, B * 8, cudaMemcpyDeviceToHost, c->stream);
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  *rc = (e == cudaSuccess) ? MSG_OK : MSG_ERR_CUDA;
   double t = 0.0;
-  for (int k = 0; k < B; ++k) t += c->hpin[k];
+  *rc = finish(c, B, 1, &t);
   return t;
 }
 

@@ -2,9 +2,9 @@
 // fused dot products, deterministic reductions and scans (B200, sm_100a).
 //
 // SpMV and the vector updates stream the DIA arrays (d, six off-diagonals) once per
-// row: 72 B/row for y = A x in FP64.  Reductions use a fixed grid of kRedBlocks
-// blocks so that the partial sums, and therefore every dot product, are identical
-// from run to run.
+// row: 72 B/row for y = A x in FP64.  One row per thread; reductions write one
+// partial per block and a fixed-order second stage (k_finish) sums them, so every
+// dot product repeats bit for bit from run to run.
 #include "msg_ctx.cuh"
 #include <cooperative_groups.h>
 #include <vector>
@@ -134,12 +134,12 @@ __global__ void __launch_bounds__(256) k_spmv(Geo3 g, const double *__restrict__
   }
   if (MODE >= 2) {
     double s = block_sum<256>(a1, sh);
-    if (threadIdx.x == 0) part[kRedBlocks + blockIdx.x] = s;
+    if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = s;
   }
 }
 
 int launch_spmv(msg_ctx *c, const double *x, double *y) {
-  k_spmv<0, false><<<kRedBlocks, 256, 0, c->stream>>>(geo3(c), c->dmat, c->lu, x, nullptr, y, nullptr, nullptr);
+  k_spmv<0, false><<<nblk(c->N), 256, 0, c->stream>>>(geo3(c), c->dmat, c->lu, x, nullptr, y, nullptr, nullptr);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) k_bicg_xr(int n, double *x, double *r, co
   double t = block_sum<256>(s0, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
   t = block_sum<256>(s1, sh);
-  if (threadIdx.x == 0) part[kRedBlocks + blockIdx.x] = t;
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = t;
 }
 
 __global__ void __launch_bounds__(256) k_dot2(int n, const double *a, const double *b, const double *cc, double *part) {
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) k_dot2(int n, const double *a, const doub
   if (threadIdx.x == 0) part[blockIdx.x] = t;
   if (cc) {
     t = block_sum<256>(s1, sh);
-    if (threadIdx.x == 0) part[kRedBlocks + blockIdx.x] = t;
+    if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = t;
   }
 }
 
@@ -268,28 +268,42 @@ static int fetch_partials(msg_ctx *c, int count) {
   MSG_CUDA(cudaStreamSynchronize(c->stream));
   return MSG_OK;
 }
-static double host_sum(const double *p, int n) {
+
+// Second reduction stage: block a sums part[a*nparts .. a*nparts + nparts) in a fixed
+// order (strided per thread, then a fixed tree), so every result repeats bit for bit.
+__global__ void __launch_bounds__(1024) k_finish(const double *part, int nparts, double *out) {
+  __shared__ double sh[1024];
+  const double *p = part + (size_t)blockIdx.x * nparts;
   double s = 0.0;
-  for (int i = 0; i < n; ++i) s += p[i];
-  return s;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s = __dadd_rn(s, p[i]);
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+int finish(msg_ctx *c, int nparts, int narr, double *out) {
+  k_finish<<<narr, 1024, 0, c->stream>>>(c->part, nparts, c->dres);
+  MSG_CHECK_LAUNCH();
+  MSG_CUDA(cudaMemcpyAsync(c->hpin, c->dres, (size_t)narr * 8, cudaMemcpyDeviceToHost, c->stream));
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int a = 0; a < narr; ++a) out[a] = c->hpin[a];
+  return MSG_OK;
 }
 
 int dot(msg_ctx *c, const double *a, const double *b, int n, double *out) {
-  k_dot2<<<kRedBlocks, 256, 0, c->stream>>>(n, a, b, nullptr, c->part);
+  k_dot2<<<nblk(n), 256, 0, c->stream>>>(n, a, b, nullptr, c->part);
   MSG_CHECK_LAUNCH();
-  int rc = fetch_partials(c, kRedBlocks);
-  if (rc) return rc;
-  *out = host_sum(c->hpin, kRedBlocks);
-  return MSG_OK;
+  return finish(c, nblk(n), 1, out);
 }
 
 int norm1(msg_ctx *c, const double *a, int n, double *out) {
-  k_norm1<<<kRedBlocks, 256, 0, c->stream>>>(n, a, c->part);
+  k_norm1<<<nblk(n), 256, 0, c->stream>>>(n, a, c->part);
   MSG_CHECK_LAUNCH();
-  int rc = fetch_partials(c, kRedBlocks);
-  if (rc) return rc;
-  *out = host_sum(c->hpin, kRedBlocks);
-  return MSG_OK;
+  return finish(c, nblk(n), 1, out);
 }
 
 int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan) {
@@ -325,13 +339,13 @@ int lam_length(msg_ctx *c, const double *dh, const double *hn, double *out) {
 }
 
 int axpby(msg_ctx *c, double *y, const double *x, double a, const double *w, int n) {
-  k_axpby<<<kRedBlocks, 256, 0, c->stream>>>(n, y, x, a, w);
+  k_axpby<<<nblk(n), 256, 0, c->stream>>>(n, y, x, a, w);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
 
 int scale(msg_ctx *c, double *y, double a, int n) {
-  k_scale<<<kRedBlocks, 256, 0, c->stream>>>(n, y, a);
+  k_scale<<<nblk(n), 256, 0, c->stream>>>(n, y, a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -483,7 +497,9 @@ int solve_bicgs(msg_ctx *c, double *x) {
   const Geo3 g = geo3(c);
   int rc;
   // r = b - A x
-  k_spmv<0, true><<<kRedBlocks, 256, 0, c->stream>>>(g, c->dmat, c->lu, x, c->rhs, c->r, nullptr, nullptr);
+  const int nb = nblk(n);
+  double red[2];
+  k_spmv<0, true><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, x, c->rhs, c->r, nullptr, nullptr);
   MSG_CHECK_LAUNCH();
   bool need_dilu = (c->prm.precon_type == 0) || c->prm.ref_quirks;
   if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
@@ -496,33 +512,33 @@ int solve_bicgs(msg_ctx *c, double *x) {
       MSG_CUDA(cudaMemcpyAsync(c->p, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
     } else {
       beta = (sk / sk0) * (alpha / omega);
-      k_bicg_p<<<kRedBlocks, 256, 0, c->stream>>>(n, c->p, c->r, c->v, beta, omega);
+      k_bicg_p<<<nb, 256, 0, c->stream>>>(n, c->p, c->r, c->v, beta, omega);
       MSG_CHECK_LAUNCH();
     }
     if ((rc = apply_prec(c, c->p, c->z))) return rc;
-    k_spmv<1, false><<<kRedBlocks, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->v, c->rs, c->part);
+    k_spmv<1, false><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->v, c->rs, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = fetch_partials(c, kRedBlocks))) return rc;
-    sk2 = host_sum(c->hpin, kRedBlocks);
+    if ((rc = finish(c, nb, 1, red))) return rc;
+    sk2 = red[0];
     alpha = sk / sk2;
-    k_bicg_xr<<<kRedBlocks, 256, 0, c->stream>>>(n, x, c->r, c->z, c->v, c->rs, alpha, c->part);
+    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, x, c->r, c->z, c->v, c->rs, alpha, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = fetch_partials(c, 2 * kRedBlocks))) return rc;
-    c->rnorm = host_sum(c->hpin, kRedBlocks);
+    if ((rc = finish(c, nb, 1, red))) return rc;
+    c->rnorm = red[0];
     c->conv_flag = (std::sqrt(c->rnorm / c->bnorm) <= c->errtol) ? 1 : 0;
     if (c->conv_flag == 1) break;
     if ((rc = apply_prec(c, c->r, c->z))) return rc;
-    k_spmv<2, false><<<kRedBlocks, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->t, c->r, c->part);
+    k_spmv<2, false><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->t, c->r, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = fetch_partials(c, 2 * kRedBlocks))) return rc;
-    ts = host_sum(c->hpin, kRedBlocks);
-    tt = host_sum(c->hpin + kRedBlocks, kRedBlocks);
+    if ((rc = finish(c, nb, 2, red))) return rc;
+    ts = red[0];
+    tt = red[1];
     omega = ts / tt;
-    k_bicg_xr<<<kRedBlocks, 256, 0, c->stream>>>(n, x, c->r, c->z, c->t, c->rs, omega, c->part);
+    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, x, c->r, c->z, c->t, c->rs, omega, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = fetch_partials(c, 2 * kRedBlocks))) return rc;
-    c->rnorm = host_sum(c->hpin, kRedBlocks);
-    double sk_next = host_sum(c->hpin + kRedBlocks, kRedBlocks);
+    if ((rc = finish(c, nb, 2, red))) return rc;
+    c->rnorm = red[0];
+    double sk_next = red[1];
     c->conv_flag = (std::sqrt(c->rnorm / c->bnorm) <= c->errtol) ? 1 : 0;
     if (c->conv_flag == 1 || c->in_iter == c->prm.maxinn_iter) break;
     sk0 = sk;

@@ -72,7 +72,7 @@ typedef struct orc {
   double *slope_rhs;         /* vector the line-search slope reads (Q2) */
   /* time module */
   double current_t, delt_old1, delt_old2;   /* current_t kept as float value (real(SP)) */
-  int timestep_num, last_conv, last_out;
+  int timestep_num, last_conv, last_out, amg_age, amg_force;
   /* statistics */
   long long n_func, n_matvec, n_prec;
 } orc_t;
@@ -448,7 +448,11 @@ static void make_matvec(orc_t *o) {
   make_matrix(o, o->lev[0].dmat, o->lev[0].lumat);
   if (o->prm.precon_type == 1) {
     if (o->prm.ref_quirks) make_amgmat(o);
-    else if (!o->prm.amg_lag || o->out_iter <= 1 || o->nlevel <= 1) own_amg_setup(o);
+    else if (!o->prm.amg_lag || o->nlevel <= 1 || o->amg_force || (o->out_iter <= 1 && o->amg_age >= o->prm.amg_lag)) {
+      own_amg_setup(o);
+      o->amg_age = 0;
+      o->amg_force = 0;
+    }
   }
   free(tmp);
 }
@@ -1102,6 +1106,7 @@ static int calc_numsol(orc_t *o, msg_stats_t *stx) {
   int n = o->ncalc, maxnun = 0, status = MSG_NEWTON_MAXIT;
   double maxunk, check_val;
   msg_stats_t st; memset(&st, 0, sizeof(st));
+  o->amg_age++;
   set_backtr(o);
   for (o->out_iter = 1; o->out_iter <= o->prm.maxout_iter; ++o->out_iter) {
     if (o->out_iter > 1) o->l2_pre = o->l2_new;
@@ -1371,7 +1376,7 @@ void orc_calc_func(void *h, const double *x, double *f) { calc_func((orc_t *)h, 
 
 void orc_make_matvec(void *h, double *dmat, double *lumat, double *rhs) {
   orc_t *o = h;
-  o->out_iter = 0;   /* a direct call always rebuilds the hierarchy */
+  o->amg_force = 1;   /* a direct call always rebuilds the hierarchy */
   make_matvec(o);
   if (dmat) memcpy(dmat, o->lev[0].dmat, 8 * o->ncalc);
   if (lumat) memcpy(lumat, o->lev[0].lumat, 8 * o->nnz);

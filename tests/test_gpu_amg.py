@@ -110,3 +110,18 @@ def test_amg_lagged_setup_parity():
     assert rg == ro == 0
     hg, ho = g.get_state()["head_new"], o.get_state()["head_new"]
     assert np.max(np.abs(hg - ho)) / np.max(np.abs(ho)) <= 1e-8
+
+
+def test_amg_lag_over_steps_parity():
+    """amg_lag = 3: one hierarchy serves three time steps; same rule in the oracle."""
+    p = make_config("hetero", shape=(32, 28, 16), seed=14)
+    ov = dict(AMG, amg_lag=3, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    from msg123_b200.solver import GpuSolver
+    g, o = GpuSolver(p, **ov), Oracle(p, **ov)
+    g.init_state(); o.init_state()
+    rg, sg = g.advance(nsteps=5)
+    ro, so = o.advance(nsteps=5)
+    assert rg == ro == 0
+    hg, ho = g.get_state()["head_new"], o.get_state()["head_new"]
+    assert np.max(np.abs(hg - ho)) / np.max(np.abs(ho)) <= 1e-8
+    print("newton GPU", sg["newton_total"], "oracle", so["newton_total"])
