@@ -261,6 +261,19 @@ MSG_API int msg_gpu_guess_rejected(msg_ctx_t *ctx);
 /* Number of kernels this library has launched in this process (all contexts). */
 MSG_API long long msg_gpu_launch_count(void);
 
+/* Launch shapes for the kernels without reductions (multiples of 32 in 32..1024):
+ * blk_cell for the van Genuchten/storage pass, blk_smooth for the level-1 Jacobi and
+ * residual passes of the V-cycle.  Chosen per grid by msg123_b200/autotune.py. */
+MSG_API int msg_gpu_set_tuning(msg_ctx_t *ctx, int32_t blk_cell, int32_t blk_smooth);
+
+/* Batched ensemble (no counterpart in the reference): advance n independent contexts by
+ * nsteps accepted steps each.  nworkers host threads take members from a shared queue
+ * and drive each on its own CUDA stream, so members of uneven size and uneven Newton
+ * counts run concurrently on the GPU.  rech_until / rech_after: per member (NULL: no
+ * schedule).  stats: n entries, may be NULL. */
+MSG_API int msg_gpu_ensemble_advance(msg_ctx_t **ctx, int32_t n, int32_t nsteps, const double *rech_until,
+                                     const double *rech_after, int32_t nworkers, msg_run_stats_t *stats);
+
 /* Enable (1) or disable (0) the per-phase CUDA-event timers (adds syncs). */
 MSG_API int msg_gpu_set_timing(msg_ctx_t *ctx, int32_t on);
 

@@ -1060,10 +1060,12 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
     return MSG_OK;
   }
   Dia D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat, c->lu};
+  const int bs = (l == 0 && c->blk_smooth > 0) ? c->blk_smooth : kThreads;
+  const int gs = (n + bs - 1) / bs;
   double *r = (l == 0) ? A->r0 : L.r;
   double *tmp = (l == 0) ? A->t0 : L.x2;
   auto sweep = [&](const double *xin, double *xout) {
-    if (l == 0) k_jac_dia<<<g, kThreads, 0, s>>>(D, b, w, xin, xout);
+    if (l == 0) k_jac_dia<<<gs, bs, 0, s>>>(D, b, w, xin, xout);
     else k_jac_csr<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, b, w, xin, xout);
   };
   // pre-smoothing: the current iterate alternates between x and tmp, so that every
@@ -1073,7 +1075,7 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
     MSG_CUDA(cudaMemsetAsync(x, 0, (size_t)n * 8, s));
   } else {
     if (sw % 2 == 0) { cur = tmp; oth = x; }
-    k_jac_first<<<g, kThreads, 0, s>>>(n, b, l == 0 ? c->dmat : L.diag, w, cur);
+    k_jac_first<<<gs, bs, 0, s>>>(n, b, l == 0 ? c->dmat : L.diag, w, cur);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
       sweep(cur, oth);
@@ -1083,14 +1085,14 @@ static int vcycle(msg_ctx *c, int l, const double *b, double *x) {
   }
   if (!last) {
     AmgLevel &C = A->lv[l + 1];
-    if (l == 0) k_res_dia<<<g, kThreads, 0, s>>>(D, b, cur, r);
+    if (l == 0) k_res_dia<<<gs, bs, 0, s>>>(D, b, cur, r);
     else k_res_csr<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, b, cur, r);
     MSG_CHECK_LAUNCH();
     k_restrict<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval, r, C.b);
     MSG_CHECK_LAUNCH();
     int rc = vcycle(c, l + 1, C.b, C.x);
     if (rc) return rc;
-    k_prolong<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval, C.x, cur);
+    k_prolong<<<gs, bs, 0, s>>>(n, C.pptr, C.pcol, C.pval, C.x, cur);
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {
@@ -1159,40 +1161,42 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   const int g = nb(n);
   Dia32 D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, c->lu_f};
   const bool single = (A->lv.size() == 1);
+  const int bs = c->blk_smooth > 0 ? c->blk_smooth : kThreads;
+  const int gs = (n + bs - 1) / bs;
   float *cur = A->x0f, *oth = A->t0f;
   if (sw == 0) {
     MSG_CUDA(cudaMemsetAsync(cur, 0, (size_t)n * 4, s));
   } else {
-    k_jac_first_f<double><<<g, kThreads, 0, s>>>(n, b, c->dmat_f, w, cur);
+    k_jac_first_f<double><<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_dia_f<float><<<g, kThreads, 0, s>>>(D, b, w, cur, oth);
+      k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, b, w, cur, oth);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!single) {
     AmgLevel &C = A->lv[1];
-    k_res_dia_f<<<g, kThreads, 0, s>>>(D, b, cur, A->r0f);
+    k_res_dia_f<<<gs, bs, 0, s>>>(D, b, cur, A->r0f);
     MSG_CHECK_LAUNCH();
     k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, 1, C.bf, C.xf);
     if (rc) return rc;
-    k_prolong_f<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
+    k_prolong_f<<<gs, bs, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {
     if (k == sw - 1) {   // the last sweep writes the FP64 output
-      k_jac_dia_f<double><<<g, kThreads, 0, s>>>(D, b, w, cur, z);
+      k_jac_dia_f<double><<<gs, bs, 0, s>>>(D, b, w, cur, z);
       MSG_CHECK_LAUNCH();
       return MSG_OK;
     }
-    k_jac_dia_f<float><<<g, kThreads, 0, s>>>(D, b, w, cur, oth);
+    k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, b, w, cur, oth);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }
-  k_f2d<<<g, kThreads, 0, s>>>(n, cur, z);
+  k_f2d<<<gs, bs, 0, s>>>(n, cur, z);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }

@@ -10,7 +10,10 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <new>
+#include <string>
+#include <thread>
 #include <vector>
 
 namespace msg {
@@ -457,6 +460,8 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
   c->newper_inv = 1.0 / c->newper;
   c->delt = p->ini_step; c->delt_inv = 1.0 / p->ini_step;
   c->last_conv = -1;
+  c->blk_cell = kThreads;
+  c->blk_smooth = kThreads;
   MSG_CUDA(cudaGetDevice(&c->device));
   {
     // keep freed stream-ordered allocations in the pool (the AMG hierarchy is rebuilt
@@ -795,6 +800,49 @@ int msg_gpu_kernel_time(msg_ctx_t *c, int32_t which, int32_t reps, double *ms_pe
   float ms = 0.f;
   MSG_CUDA(cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]));
   *ms_per_launch = (double)ms / reps;
+  return MSG_OK;
+}
+
+int msg_gpu_set_tuning(msg_ctx_t *c, int32_t blk_cell, int32_t blk_smooth) {
+  auto ok = [](int b) { return b >= 32 && b <= 1024 && (b % 32) == 0; };
+  if (!c || !ok(blk_cell) || !ok(blk_smooth)) { set_error("set_tuning: block sizes must be multiples of 32 in 32..1024"); return MSG_ERR_ARG; }
+  c->blk_cell = blk_cell;
+  c->blk_smooth = blk_smooth;
+  return MSG_OK;
+}
+
+// Ensemble driver: worker threads take members from a shared queue and advance each
+// for nsteps accepted steps on the member's own stream, so members of uneven size and
+// uneven Newton counts keep the GPU busy together.
+int msg_gpu_ensemble_advance(msg_ctx_t **ctx, int32_t n, int32_t nsteps, const double *rech_until,
+                             const double *rech_after, int32_t nworkers, msg_run_stats_t *stats) {
+  if (!ctx || n < 1 || nsteps < 0 || nworkers < 1) return MSG_ERR_ARG;
+  for (int k = 0; k < n; ++k) if (!ctx[k]) return MSG_ERR_ARG;
+  int dev = 0;
+  MSG_CUDA(cudaGetDevice(&dev));
+  std::atomic<int> next(0), err(0);
+  std::vector<std::string> msgs(n);
+  auto work = [&]() {
+    cudaSetDevice(dev);
+    for (;;) {
+      int k = next.fetch_add(1);
+      if (k >= n) return;
+      msg_run_stats_t st;
+      memset(&st, 0, sizeof(st));
+      int rc = advance(ctx[k], nsteps, rech_until ? rech_until[k] : 1.0e30, rech_after ? rech_after[k] : 1.0, &st);
+      if (rc < 0) { err.store(rc); msgs[k] = get_error(); }
+      if (stats) stats[k] = st;
+    }
+  };
+  int nw = std::min<int>(nworkers, n);
+  std::vector<std::thread> pool;
+  for (int w = 0; w < nw; ++w) pool.emplace_back(work);
+  for (auto &t : pool) t.join();
+  if (err.load() < 0) {
+    for (int k = 0; k < n; ++k)
+      if (!msgs[k].empty()) { set_error("ensemble member %d: %s", k, msgs[k].c_str()); break; }
+    return err.load();
+  }
   return MSG_OK;
 }
 

@@ -74,6 +74,9 @@ struct msg_ctx {
   cudaEvent_t ev[8];
   double t_ms[5];
   int timing;
+  // ---- launch shapes chosen by the autotuner (kernels without reductions only) ---------------
+  int blk_cell;      // block size of the van Genuchten / storage pass (k_cell)
+  int blk_smooth;    // block size of the level-1 Jacobi / residual passes of the V-cycle
 };
 
 namespace msg {

@@ -515,7 +515,8 @@ static CellArgs cell_args(msg_ctx *c, const double *h) {
 }
 
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
-  k_cell<false><<<nblk(c->N), kThreads, 0, c->stream>>>(c->N, cell_args(c, h));
+  const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
+  k_cell<false><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, h));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, h);
   a.F = F;
@@ -526,7 +527,8 @@ int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
 }
 
 int launch_make_matvec(msg_ctx *c) {
-  k_cell<true><<<nblk(c->N), kThreads, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
+  const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
+  k_cell<true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, c->head_new);
   a.F = c->rhs;

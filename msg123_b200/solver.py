@@ -62,6 +62,7 @@ def load_library():
     L.msg_gpu_timers.argtypes = [vp, abi.PD]
     L.msg_gpu_set_timing.argtypes = [vp, C.c_int32]
     L.msg_gpu_kernel_time.argtypes = [vp, C.c_int32, C.c_int32, abi.PD]
+    L.msg_gpu_set_tuning.argtypes = [vp, C.c_int32, C.c_int32]
     L.msg_gpu_amg_nlevel.argtypes = [vp]
     L.msg_gpu_amg_level_sizes.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PI]
     L.msg_gpu_amg_level.argtypes = [vp, C.c_int32, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
@@ -251,6 +252,9 @@ class GpuSolver:
 
     def set_timing(self, on=True):
         _check(load_library().msg_gpu_set_timing(self.h, int(bool(on))), "set_timing")
+
+    def set_tuning(self, blk_cell, blk_smooth):
+        _check(load_library().msg_gpu_set_tuning(self.h, int(blk_cell), int(blk_smooth)), "set_tuning")
 
     def kernel_time(self, which, reps=20):
         ms = C.c_double()
