@@ -46,9 +46,11 @@ __global__ void k_extrap(int n, double *h, const double *h_old, const double *h_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     h[i] = __dadd_rn(h_old[i], __dmul_rn(ratio, __dsub_rn(h_old[i], h_old2[i])));
 }
+// out = -(f2 - f1) / eps; with NEG the caller passes g = -f1, and f2 - f1 = f2 + g exactly.
+template <bool NEG>
 __global__ void k_vecjac_out(int n, double *out, const double *f2, const double *f1, double eps_inv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = __dmul_rn(-__dsub_rn(f2[i], f1[i]), eps_inv);
+    out[i] = __dmul_rn(-(NEG ? __dadd_rn(f2[i], f1[i]) : __dsub_rn(f2[i], f1[i])), eps_inv);
 }
 __global__ void k_to_f32(size_t n, const double *a, float *b) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -76,6 +78,7 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
   int rc = launch_calc_func(c, h, F, true);
   if (rc) return rc;
   *l2 = sum_part(c, nblk(c->N), &rc);   // synchronises the stream
+  c->l2_last = *l2;
   if (c->timing) {
     cudaEventRecord(c->ev[0], c->stream);
     cudaEventSynchronize(c->ev[0]);
@@ -133,13 +136,20 @@ static int solve_linalg(msg_ctx *c, double init_norm, double *x, double *last_no
   return MSG_OK;
 }
 
-// calc_vecjacf (Calc_function.f90:515-621)
-static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out) {
+// calc_vecjacf (Calc_function.f90:515-621).  neg_f1, when given, is -F(x) already at hand:
+// the make_matvec right-hand side of the iterate x it was assembled at, whose arithmetic is
+// that of calc_func term for term, so the finite difference is the same bit for bit and
+// one residual evaluation is saved.
+static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out, const double *neg_f1 = nullptr) {
   const int n = c->N;
-  double *f1 = c->v, *f2 = c->t, *jc = c->z;
+  const double *f1 = neg_f1;
+  double *f2 = c->t, *jc = c->z;
   int rc;
   double dummy;
-  if ((rc = func_norm(c, x, f1, &dummy))) return rc;
+  if (!f1) {
+    if ((rc = func_norm(c, x, c->v, &dummy))) return rc;
+    f1 = c->v;
+  }
   double l2_v, l2_x, l1_v;
   if ((rc = dot(c, v, v, n, &l2_v))) return rc;
   if ((rc = dot(c, x, v, n, &l2_x))) return rc;
@@ -149,7 +159,8 @@ static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out) {
   double eps_inv = 1.0 / eps;
   if ((rc = axpby(c, jc, x, eps, v, n))) return rc;
   if ((rc = func_norm(c, jc, f2, &dummy))) return rc;
-  k_vecjac_out<<<nblk(n), 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
+  if (neg_f1) k_vecjac_out<true><<<nblk(n), 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
+  else k_vecjac_out<false><<<nblk(n), 256, 0, c->stream>>>(n, out, f2, f1, eps_inv);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -168,12 +179,15 @@ static int run_backtr(msg_ctx *c) {
   double temp_lam, rhs1, rhs2, lam_inv, lam2_inv, del_lam, av, bv, root, lam_max, lam_base, lam_diff, lam_incr;
   int rc;
   c->lam = 1.0;
+  // J.dh by finite differences at the iterate the system was assembled at (rhs = -F there),
+  // taken before F(head_new) so that the last residual evaluation of the line search is
+  // always the one at the accepted head_new (its S and kr stay current; calc_numsol reuses it)
+  double *jacvec = c->tmpv;
+  if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) return rc;
   double dummy;
   if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
   double l2_pnorm;
   if ((rc = dot(c, c->head_change, c->head_change, n, &l2_pnorm))) return rc;
-  double *jacvec = c->tmpv;
-  if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec))) return rc;
   double sql2_pnorm = std::sqrt(l2_pnorm);
   if (sql2_pnorm > c->maxstep) {
     maxpnorm = c->maxstep / sql2_pnorm;
@@ -314,8 +328,10 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
       status = MSG_NAN;
       break;
     }
+    bool evaluated = false;   // F(head_new) and its norm already computed by the line search
     if (c->conv_flag != 1) {
       if ((rc = run_backtr(c))) return rc;
+      evaluated = true;
       if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
       check_val = std::fabs(c->maxvar) * c->len_scal;
       maxunk = std::fabs(maxunk) * c->len_scal;
@@ -324,7 +340,8 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
       else if (check_val <= crit && maxunk < XMAX) c->conv_flag = 1;
       if (c->conv_flag != 1 && c->back_flag != 1) set_eater(c);
     }
-    if ((rc = func_norm(c, c->head_new, c->new_f, &c->l2_new))) return rc;
+    if (evaluated) c->l2_new = c->l2_last;
+    else if ((rc = func_norm(c, c->head_new, c->new_f, &c->l2_new))) return rc;
     st.back_total += c->back_iter; st.back_iter_last = c->back_iter;
     double conv_var = c->maxvar * c->len_scal;
     if (c->conv_flag == 1) {

@@ -63,6 +63,7 @@ struct msg_ctx {
   // ---- Newton module variables (Nonlinear_solution.f90:24-27) ---------------------------------
   int back_iter, back_flag, beta_iter, in_iter, conv_flag, out_iter;
   double maxvar, l2_new, l2_pre, l2_jnorm, lam, eta, gradient, maxstep, errtol, bnorm, rnorm;
+  double l2_last;    // squared norm of the last residual evaluated through func_norm
   // ---- time loop ---------------------------------------------------------------------------------
   double current_t, delt_old1, delt_old2;
   int timestep_num, last_conv, last_out;
