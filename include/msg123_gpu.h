@@ -246,6 +246,9 @@ MSG_API int msg_gpu_cnn_collect(msg_cnn_t *cnn, msg_ctx_t *ctx);
 MSG_API int msg_gpu_cnn_nsamples(msg_cnn_t *cnn);
 /* append a sample from host arrays: x [N][16] features, y [N] target, N = nx*ny*nz */
 MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *cnn, int32_t nx, int32_t ny, int32_t nz, const float *x, const float *y);
+/* inference pass of the tensor-core (tcgen05) path on a stored sample; out: N floats.
+   No reference counterpart (the learned guess is an addition of this library). */
+MSG_API int msg_gpu_cnn_infer(msg_cnn_t *cnn, int32_t sample, float *out);
 /* mean squared error on one sample; grad (msg_gpu_cnn_nparam floats) and out (N) may be NULL */
 MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *cnn, int32_t sample, double *loss, float *grad, float *out);
 /* AdamW training over the stored samples */

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmsg123gpu.so")
-SOURCES = ["msg_api.cu", "msg_physics.cu", "msg_linear.cu", "msg_amg.cu", "msg_learned.cu"]
+SOURCES = ["msg_api.cu", "msg_physics.cu", "msg_linear.cu", "msg_amg.cu", "msg_learned.cu", "msg_conv_tc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 

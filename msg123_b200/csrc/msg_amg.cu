@@ -60,6 +60,12 @@ struct AmgState {
   double *tdm = nullptr;
   // mixed precision level-1 images
   float *d1f = nullptr, *lu1f = nullptr;
+  // Device arena for everything one hierarchy build allocates (levels, transfer operators,
+  // Galerkin temporaries): a bump pointer reset at each rebuild, so rebuilds never go to
+  // the allocator.  A build that outgrows it takes the rest from the stream-ordered pool
+  // and the arena is enlarged before the next build.
+  char *arena = nullptr;
+  size_t arena_cap = 0, arena_used = 0, arena_spill = 0;
 };
 
 static AmgState *S(msg_ctx *c) { return reinterpret_cast<AmgState *>(c->amg); }
@@ -733,10 +739,33 @@ __global__ void k_col0(int nnz, const int *offrow1, int *col0) {
 // ---------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------
-static void free_level(AmgLevel &L, cudaStream_t s) {
+// Allocation of one hierarchy build: from the arena, else (arena full) from the pool.
+template <typename T>
+static int halloc(msg_ctx *c, T **p, size_t n) {
+  AmgState *A = S(c);
+  const size_t bytes = ((n ? n : 1) * sizeof(T) + 255) & ~(size_t)255;
+  if (A->arena && A->arena_used + bytes <= A->arena_cap) {
+    *p = reinterpret_cast<T *>(A->arena + A->arena_used);
+    A->arena_used += bytes;
+    return MSG_OK;
+  }
+  A->arena_spill += bytes;
+  MSG_CUDA(cudaMallocAsync((void **)p, bytes, c->stream));
+  return MSG_OK;
+}
+
+// Release a pointer from halloc: arena memory is reclaimed at the next reset.
+static void hfree(AmgState *A, void *q, cudaStream_t s) {
+  if (!q) return;
+  const char *b = reinterpret_cast<const char *>(q);
+  if (A->arena && b >= A->arena && b < A->arena + A->arena_cap) return;
+  cudaFreeAsync(q, s);
+}
+
+static void free_level(AmgState *A, AmgLevel &L, cudaStream_t s) {
   void *p[] = {L.rowptr, L.col, L.diag, L.val, L.pptr, L.pcol, L.pval, L.rptr, L.rcol, L.rval, L.agg, L.cinv,
                L.x, L.b, L.r, L.x2, L.diag_f, L.val_f, L.pval_f, L.rval_f, L.val_h, L.xf, L.bf, L.rf, L.x2f};
-  for (void *q : p) if (q) cudaFreeAsync(q, s);
+  for (void *q : p) hfree(A, q, s);
   L = AmgLevel();
 }
 
@@ -786,9 +815,9 @@ static int spgemm(msg_ctx *c, AmgState *A, int nrows, const int *ap, const int *
   int rc;
   int *cnt = nullptr, *longrows = nullptr, *nl = nullptr;
   *ovf = 0;
-  if ((rc = dalloc(c, &cnt, nrows + 1))) return rc;
-  if ((rc = dalloc(c, &longrows, nrows + 1))) return rc;
-  if ((rc = dalloc(c, &nl, 2))) return rc;
+  if ((rc = halloc(c, &cnt, nrows + 1))) return rc;
+  if ((rc = halloc(c, &longrows, nrows + 1))) return rc;
+  if ((rc = halloc(c, &nl, 2))) return rc;
   MSG_CUDA(cudaMemsetAsync(nl, 0, 8, s));
   k_spgemm_t<0><<<(nrows + 127) / 128, 128, 0, s>>>(nrows, ap, ac, av, adiag, bp, bc, bv, split_diag, cnt, nullptr,
                                                    nullptr, nullptr, nullptr, longrows, nl);
@@ -803,18 +832,18 @@ static int spgemm(msg_ctx *c, AmgState *A, int nrows, const int *ap, const int *
         nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, cnt, nullptr, nullptr, nullptr, nullptr, A->cnt, longrows);
     MSG_CHECK_LAUNCH();
   }
-  if ((rc = dalloc(c, cptr, nrows + 1))) return rc;
+  if ((rc = halloc(c, cptr, nrows + 1))) return rc;
   int tot = 0;
   if ((rc = scan_exclusive(c, cnt, *cptr, nrows, &tot))) return rc;
   if ((rc = read_counter(c, A, ovf))) return rc;
   if (*ovf) {
-    cudaFreeAsync(cnt, s); cudaFreeAsync(longrows, s); cudaFreeAsync(nl, s); cudaFreeAsync(*cptr, s);
+    hfree(S(c), cnt, s); hfree(S(c), longrows, s); hfree(S(c), nl, s); hfree(S(c), *cptr, s);
     *cptr = nullptr;
     return MSG_OK;
   }
   MSG_CUDA(cudaMemcpyAsync(*cptr + nrows, &tot, 4, cudaMemcpyHostToDevice, s));
-  if ((rc = dalloc(c, ccol, tot))) return rc;
-  if ((rc = dalloc(c, cval, tot))) return rc;
+  if ((rc = halloc(c, ccol, tot))) return rc;
+  if ((rc = halloc(c, cval, tot))) return rc;
   k_spgemm_t<1><<<(nrows + 127) / 128, 128, 0, s>>>(nrows, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr,
                                                    *ccol, *cval, cdiag, nullptr, nullptr);
   MSG_CHECK_LAUNCH();
@@ -823,7 +852,7 @@ static int spgemm(msg_ctx *c, AmgState *A, int nrows, const int *ap, const int *
         nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr, *ccol, *cval, cdiag, A->cnt, longrows);
     MSG_CHECK_LAUNCH();
   }
-  cudaFreeAsync(cnt, s); cudaFreeAsync(longrows, s); cudaFreeAsync(nl, s);
+  hfree(S(c), cnt, s); hfree(S(c), longrows, s); hfree(S(c), nl, s);
   *cnnz = tot;
   return MSG_OK;
 }
@@ -869,7 +898,7 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   if (nc == 0 || nc >= n) return MSG_OK;
   AmgLevel C;
   C.n = nc;
-  if ((rc = dalloc(c, &C.agg, n))) return rc;
+  if ((rc = halloc(c, &C.agg, n))) return rc;
   k_agg_a<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->st, A->aggid, A->agg2, lv);
   MSG_CHECK_LAUNCH();
   k_agg_b<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->agg2, C.agg, lv);
@@ -881,36 +910,36 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   {
     int ovp = 0;
     if ((rc = read_counter(c, A, &ovp))) return rc;
-    if (ovp) { free_level(C, s); return MSG_OK; }
+    if (ovp) { free_level(A, C, s); return MSG_OK; }
   }
-  if ((rc = dalloc(c, &C.pptr, n + 1))) return rc;
+  if ((rc = halloc(c, &C.pptr, n + 1))) return rc;
   int pnnz = 0;
   if ((rc = scan_exclusive(c, A->tmpi, C.pptr, n, &pnnz))) return rc;
   MSG_CUDA(cudaMemcpyAsync(C.pptr + n, &pnnz, 4, cudaMemcpyHostToDevice, s));
   C.pnnz = pnnz;
-  if ((rc = dalloc(c, &C.pcol, pnnz))) return rc;
-  if ((rc = dalloc(c, &C.pval, pnnz))) return rc;
+  if ((rc = halloc(c, &C.pcol, pnnz))) return rc;
+  if ((rc = halloc(c, &C.pval, pnnz))) return rc;
   k_p_fill<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, F.val, A->sflag, C.agg, A->tdm, (double)c->prm.jac_omega,
                                       C.pptr, C.pcol, C.pval);
   MSG_CHECK_LAUNCH();
   // R = P^T
   int *rcnt = nullptr;
-  if ((rc = dalloc(c, &rcnt, nc + 1))) return rc;
+  if ((rc = halloc(c, &rcnt, nc + 1))) return rc;
   MSG_CUDA(cudaMemsetAsync(rcnt, 0, (size_t)(nc + 1) * 4, s));
   k_r_count<<<nb(pnnz), kThreads, 0, s>>>(pnnz, C.pcol, rcnt);
   MSG_CHECK_LAUNCH();
-  if ((rc = dalloc(c, &C.rptr, nc + 1))) return rc;
+  if ((rc = halloc(c, &C.rptr, nc + 1))) return rc;
   int rn = 0;
   if ((rc = scan_exclusive(c, rcnt, C.rptr, nc, &rn))) return rc;
   MSG_CUDA(cudaMemcpyAsync(C.rptr + nc, &rn, 4, cudaMemcpyHostToDevice, s));
-  if ((rc = dalloc(c, &C.rcol, pnnz))) return rc;
-  if ((rc = dalloc(c, &C.rval, pnnz))) return rc;
+  if ((rc = halloc(c, &C.rcol, pnnz))) return rc;
+  if ((rc = halloc(c, &C.rval, pnnz))) return rc;
   MSG_CUDA(cudaMemsetAsync(rcnt, 0, (size_t)(nc + 1) * 4, s));
   k_r_fill<<<nb(n), kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval, C.rptr, rcnt, C.rcol, C.rval);
   MSG_CHECK_LAUNCH();
   k_r_sort<<<(nc + 3) / 4, 128, 0, s>>>(nc, C.rptr, C.rcol, C.rval);
   MSG_CHECK_LAUNCH();
-  cudaFreeAsync(rcnt, s);
+  hfree(A, rcnt, s);
   // AP = A*P (diagonal first)
   int *apptr = nullptr, *apcol = nullptr;
   double *apval = nullptr;
@@ -918,20 +947,20 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   if ((rc = spgemm(c, A, n, F.rowptr, F.col, F.val, F.diag, C.pptr, C.pcol, C.pval, 0, &apptr, &apcol, &apval,
                    nullptr, &apn, &ovf)))
     return rc;
-  if (ovf) { free_level(C, s); return MSG_OK; }
+  if (ovf) { free_level(A, C, s); return MSG_OK; }
   // A_c = R * AP, diagonal split off
-  if ((rc = dalloc(c, &C.diag, nc))) return rc;
+  if ((rc = halloc(c, &C.diag, nc))) return rc;
   int cn = 0;
   if ((rc = spgemm(c, A, nc, C.rptr, C.rcol, C.rval, nullptr, apptr, apcol, apval, 1, &C.rowptr, &C.col, &C.val,
                    C.diag, &cn, &ovf)))
     return rc;
-  cudaFreeAsync(apptr, s); cudaFreeAsync(apcol, s); cudaFreeAsync(apval, s);
-  if (ovf) { free_level(C, s); return MSG_OK; }
+  hfree(A, apptr, s); hfree(A, apcol, s); hfree(A, apval, s);
+  if (ovf) { free_level(A, C, s); return MSG_OK; }
   C.nnz = cn;
-  if ((rc = dalloc(c, &C.x, nc))) return rc;
-  if ((rc = dalloc(c, &C.b, nc))) return rc;
-  if ((rc = dalloc(c, &C.r, nc))) return rc;
-  if ((rc = dalloc(c, &C.x2, nc))) return rc;
+  if ((rc = halloc(c, &C.x, nc))) return rc;
+  if ((rc = halloc(c, &C.b, nc))) return rc;
+  if ((rc = halloc(c, &C.r, nc))) return rc;
+  if ((rc = halloc(c, &C.x2, nc))) return rc;
   A->lv.push_back(C);
   *made = 1;
   return MSG_OK;
@@ -942,9 +971,9 @@ static int dense_inverse(msg_ctx *c, AmgLevel &L) {
   cudaStream_t s = c->stream;
   double *M = nullptr;
   int *piv = nullptr;
-  if ((rc = dalloc(c, &M, (size_t)n * 2 * n))) return rc;
-  if ((rc = dalloc(c, &piv, 1))) return rc;
-  if ((rc = dalloc(c, &L.cinv, (size_t)n * n))) return rc;
+  if ((rc = halloc(c, &M, (size_t)n * 2 * n))) return rc;
+  if ((rc = halloc(c, &piv, 1))) return rc;
+  if ((rc = halloc(c, &L.cinv, (size_t)n * n))) return rc;
   k_dense_fill<<<n, 256, 0, s>>>(n, L.rowptr, L.col, L.val, L.diag, M);
   MSG_CHECK_LAUNCH();
   if (n <= 1024) {
@@ -962,8 +991,8 @@ static int dense_inverse(msg_ctx *c, AmgLevel &L) {
   }
   k_dense_extract<<<n, 256, 0, s>>>(n, M, L.cinv);
   MSG_CHECK_LAUNCH();
-  cudaFreeAsync(M, s);
-  cudaFreeAsync(piv, s);
+  hfree(S(c), M, s);
+  hfree(S(c), piv, s);
   return MSG_OK;
 }
 
@@ -971,13 +1000,14 @@ void amg_free(msg_ctx *c) {
   AmgState *A = S(c);
   if (!A) return;
   cudaStream_t s = c->stream;
-  for (size_t l = 1; l < A->lv.size(); ++l) free_level(A->lv[l], s);
+  for (size_t l = 1; l < A->lv.size(); ++l) free_level(A, A->lv[l], s);
   A->lv.clear();
   void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t1, A->t2,
                A->tdm, A->d1f, A->lu1f};
   for (void *q : p) if (q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
   if (A->hcnt) cudaFreeHost(A->hcnt);
+  if (A->arena) cudaFree(A->arena);
   delete A;
   c->amg = nullptr;
 }
@@ -1003,8 +1033,23 @@ int amg_setup(msg_ctx *c) {
     k_col0<<<nb(c->nnz), kThreads, 0, s>>>(c->nnz, c->offrow, A->col0);
     MSG_CHECK_LAUNCH();
   }
-  for (size_t l = 1; l < A->lv.size(); ++l) free_level(A->lv[l], s);
+  for (size_t l = 1; l < A->lv.size(); ++l) free_level(A, A->lv[l], s);
   A->lv.clear();
+  // reset the arena; enlarge it first when the previous build did not fit
+  if (A->arena_spill) {
+    const size_t need = A->arena_used + A->arena_spill;
+    if (A->arena) {
+      MSG_CUDA(cudaStreamSynchronize(s));
+      cudaFree(A->arena);
+      A->arena = nullptr;
+      A->arena_cap = 0;
+    }
+    const size_t cap = ((need + need / 4) + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
+    if (cudaMalloc((void **)&A->arena, cap) == cudaSuccess) A->arena_cap = cap;
+    else { A->arena = nullptr; cudaGetLastError(); }   // keep using the pool
+  }
+  A->arena_used = 0;
+  A->arena_spill = 0;
   if ((rc = launch_dia_to_csr(c, A->val0))) return rc;
   AmgLevel L0;
   L0.n = c->N; L0.nnz = c->nnz; L0.rowptr = c->offind; L0.col = A->col0; L0.diag = c->dmat; L0.val = A->val0;
@@ -1022,14 +1067,14 @@ int amg_setup(msg_ctx *c) {
     for (size_t l = 1; l < A->lv.size(); ++l) {
       AmgLevel &L = A->lv[l];
       int nf = A->lv[l - 1].n;
-      if ((rc = dalloc(c, &L.diag_f, L.n))) return rc;
-      if ((rc = dalloc(c, &L.val_h, L.nnz))) return rc;
-      if ((rc = dalloc(c, &L.pval_f, L.pnnz))) return rc;
-      if ((rc = dalloc(c, &L.rval_f, L.pnnz))) return rc;
-      if ((rc = dalloc(c, &L.xf, L.n))) return rc;
-      if ((rc = dalloc(c, &L.bf, L.n))) return rc;
-      if ((rc = dalloc(c, &L.rf, L.n))) return rc;
-      if ((rc = dalloc(c, &L.x2f, L.n))) return rc;
+      if ((rc = halloc(c, &L.diag_f, L.n))) return rc;
+      if ((rc = halloc(c, &L.val_h, L.nnz))) return rc;
+      if ((rc = halloc(c, &L.pval_f, L.pnnz))) return rc;
+      if ((rc = halloc(c, &L.rval_f, L.pnnz))) return rc;
+      if ((rc = halloc(c, &L.xf, L.n))) return rc;
+      if ((rc = halloc(c, &L.bf, L.n))) return rc;
+      if ((rc = halloc(c, &L.rf, L.n))) return rc;
+      if ((rc = halloc(c, &L.x2f, L.n))) return rc;
       int g = std::min(nb(std::max(L.nnz, L.pnnz)), kRedBlocks * 4);
       k_d2f<<<std::min(nb(L.n), kRedBlocks * 4), kThreads, 0, s>>>(L.n, L.diag, L.diag_f);
       MSG_CHECK_LAUNCH();

@@ -89,11 +89,12 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
   return rc;
 }
 
-// make_matvec (Make_linearsystem.f90:24-68) + AMG setup when requested.
-static int make_matvec(msg_ctx *c, double *l2_rhs) {
+// make_matvec (Make_linearsystem.f90:24-68) + AMG setup when requested.  reuse: the last
+// residual evaluation was at head_new (true from the second Newton iteration on).
+static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse) {
   cudaEvent_t *ev = c->ev;
   if (c->timing) cudaEventRecord(ev[0], c->stream);
-  int rc = launch_make_matvec(c);
+  int rc = launch_make_matvec(c, reuse);
   if (rc) return rc;
   double s = sum_part(c, nblk(c->N), &rc);
   if (rc) return rc;
@@ -307,7 +308,10 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     if (c->out_iter > 1) c->l2_pre = c->l2_new;
     c->back_flag = 0; c->back_iter = 0; c->beta_iter = 0;
     double l2r;
-    if ((rc = make_matvec(c, &l2r))) return rc;
+    // from the second iteration on, the previous iteration ended with F evaluated at
+    // head_new (line search or the closing evaluation), leaving S, kr and the storage
+    // term there in srat_new / kr / sto
+    if ((rc = make_matvec(c, &l2r, c->out_iter > 1))) return rc;
     if ((rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
     if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }
     if ((rc = copy_d2d(c, c->head_pre, c->head_new, n))) return rc;
@@ -663,7 +667,7 @@ int msg_gpu_make_matvec(msg_ctx_t *c, double *dmat, double *lumat, double *rhs) 
   if (!c) return MSG_ERR_ARG;
   c->amg_force = 1;   // a direct call always rebuilds the hierarchy
   double l2;
-  int rc = make_matvec(c, &l2);
+  int rc = make_matvec(c, &l2, false);
   if (rc) return rc;
   size_t N = c->N;
   if (lumat) {
@@ -791,12 +795,21 @@ long long msg_gpu_launch_count(void) { return __atomic_load_n(&g_launches, __ATO
 // Time `reps` back-to-back launches of one kernel class on the context's stream
 // with CUDA events (the state of the last step is used as input):
 // 0 = stencil SpMV (FP64 DIA), 1 = calc_func (vG pass + flux pass),
-// 2 = make_matvec (vG pair + assembly), 3 = preconditioner apply, 4 = AMG setup.
+// 2 = make_matvec (vG pair + assembly), 3 = preconditioner apply, 4 = AMG setup,
+// 5 = the four tensor-core convolutions of the learned guess (needs an attached network).
 int msg_gpu_kernel_time(msg_ctx_t *c, int32_t which, int32_t reps, double *ms_per_launch) {
   if (!c || reps < 1 || !ms_per_launch) return MSG_ERR_ARG;
   int rc = MSG_OK;
   if (which == 3 && (c->prm.precon_type == 0 || c->prm.ref_quirks)) {
     if ((rc = launch_precon_dilu(c))) return rc;
+  }
+  if (which == 5) {
+    if (!learned_ready(c) || c->timestep_num < 1) {
+      set_error("kernel_time 5: no network attached or no previous time level");
+      return MSG_ERR_STATE;
+    }
+    const float *o = nullptr;
+    if ((rc = learned_forward(c, &o, nullptr, nullptr))) return rc;   // features into the padded buffer
   }
   auto one = [&]() -> int {
     switch (which) {
@@ -805,6 +818,7 @@ int msg_gpu_kernel_time(msg_ctx_t *c, int32_t which, int32_t reps, double *ms_pe
       case 2: return launch_make_matvec(c);
       case 3: return apply_prec(c, c->rhs, c->z);
       case 4: return (c->prm.precon_type == 1 && !c->prm.ref_quirks) ? amg_setup(c) : MSG_OK;
+      case 5: return learned_convs(c);
       default: return MSG_ERR_ARG;
     }
   };
@@ -817,6 +831,7 @@ int msg_gpu_kernel_time(msg_ctx_t *c, int32_t which, int32_t reps, double *ms_pe
   float ms = 0.f;
   MSG_CUDA(cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]));
   *ms_per_launch = (double)ms / reps;
+  if (which == 5) return learned_check(c);
   return MSG_OK;
 }
 

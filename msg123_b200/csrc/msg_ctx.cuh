@@ -87,8 +87,9 @@ int build_connectivity(msg_ctx *c, const msg_grid_t *g);
 int launch_srat_rperm(msg_ctx *c, const double *h, double pertur, double *srat, double *kr, double *alp);
 // F = calc_func(h); also writes srat_new and kr (rel_perm).  partial sums of F^2 in c->part[0..].
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm);
-// make_matvec at c->head_new: dmat, lu (DIA), rhs = -F.
-int launch_make_matvec(msg_ctx *c);
+// make_matvec at c->head_new: dmat, lu (DIA), rhs = -F.  reuse: srat_new, kr and sto
+// already hold the values at head_new (the last calc_func was evaluated there).
+int launch_make_matvec(msg_ctx *c, bool reuse = false);
 // Export the DIA Jacobian into the reference CSR order.
 int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
 int launch_mass(msg_ctx *c, double *out9_dev);
@@ -117,6 +118,11 @@ void amg_free(msg_ctx *c);
 // ---- msg_learned.cu ------------------------------------------------------------------------------
 bool learned_ready(msg_ctx *c);
 int learned_guess(msg_ctx *c);
+// features + tensor-core forward pass of the attached network (no state change)
+int learned_forward(msg_ctx *c, const float **out, double *s_out, double *ratio_out);
+// the four convolutions again on the features of the last learned_forward (timing)
+int learned_convs(msg_ctx *c);
+int learned_check(msg_ctx *c);   // sync + status of the last tensor-core pass
 void learned_free(msg_ctx *c);
 
 // ---- preconditioner dispatch (msg_linear.cu) ---------------------------------------------------------

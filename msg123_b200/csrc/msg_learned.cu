@@ -8,13 +8,16 @@
 // extrapolation:  h_{t+1} = h_t + r (h_t - h_{t-1}) + s o,  s = rms(h_t - h_{t-1}),
 // r = dt_new / dt_old, so an untrained (zero) head gives the extrapolation back.
 //
-// The convolutions are implicit GEMMs on the tensor cores with mma.sync m16n8k16
-// (BF16 x BF16 -> FP32): a warp owns 16 consecutive cells (the M dimension), the
-// 16 output channels are two n8 tiles, and each of the 27 taps is one k16 step over
-// the 16 input channels.  The input-gradient pass is the same kernel with the taps
-// mirrored and the weights transposed; the weight gradient reduces dz^T a over cells
-// with the same instruction.
+// Inference inside the time loop (learned_guess) runs the convolutions on the tcgen05
+// tensor cores with TMA-staged halo tiles and TMEM accumulators (msg_conv_tc.cu).
+// Training (forward with saved pre-activations, input and weight gradients) uses
+// implicit GEMMs with mma.sync m16n8k16 (BF16 x BF16 -> FP32): a warp owns 16
+// consecutive cells (the M dimension), the 16 output channels are two n8 tiles, and
+// each of the 27 taps is one k16 step over the 16 input channels.  The input-gradient
+// pass is the same kernel with the taps mirrored and the weights transposed; the weight
+// gradient reduces dz^T a over cells with the same instruction.
 #include "msg_ctx.cuh"
+#include "msg_conv_tc.cuh"
 #include <cuda_bf16.h>
 #include <vector>
 #include <cmath>
@@ -41,6 +44,8 @@ struct Net {
   float *w32 = nullptr;                // [kNParam] master weights
   __nv_bfloat16 *w16 = nullptr;        // [kLayers][kWl]  W[tap][co][ci]
   __nv_bfloat16 *wt16 = nullptr;       // [kLayers][kWl]  mirrored taps, transposed
+  __nv_bfloat16 *wtc = nullptr;        // [kLayers][kTaps][2][16][8] tensor-core operand layout
+  ConvPlan *plan = nullptr;            // padded activations + TMA maps of the inference grid
   float *m = nullptr, *v = nullptr, *grad = nullptr;
   float *part = nullptr;               // weight-gradient partials
   int part_cap = 0;
@@ -279,7 +284,10 @@ struct FeatArgs {
   double len_scal, inv_s, ratio;
 };
 
-__global__ void k_features(FeatArgs f, __nv_bfloat16 *x) {
+// PAD = false: compact [N][16]; PAD = true: the padded chunk-planar layout of ConvPlan
+// (plane = padded cells per chunk plane).
+template <bool PAD>
+__global__ void k_features(FeatArgs f, __nv_bfloat16 *x, long long plane) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= f.g.N) return;
   float v[kC];
@@ -292,9 +300,19 @@ __global__ void k_features(FeatArgs f, __nv_bfloat16 *x) {
   v[4] = (f.retn[i] - 1.9f) / 0.4f;
   if (i < f.g.nxy) v[5] = (f.rech_base[i] != 0.0) ? (float)(f.calc_rech[i] / f.rech_base[i]) : 0.f;
   v[6] = (float)f.ratio;
-  __nv_bfloat16 *q = x + (size_t)i * kC;
+  __align__(16) __nv_bfloat16 q[kC];
 #pragma unroll
   for (int c = 0; c < kC; ++c) q[c] = __float2bfloat16(v[c]);
+  uint4 *dst = reinterpret_cast<uint4 *>(x);
+  if (PAD) {
+    int iz = i / f.g.nxy, rem = i - iz * f.g.nxy, iy = rem / f.g.nx, ix = rem - iy * f.g.nx;
+    long long p = ((long long)(iz + 1) * (f.g.ny + 2) + (iy + 1)) * (f.g.nx + 2) + (ix + 1);
+    dst[p] = reinterpret_cast<const uint4 *>(q)[0];
+    dst[plane + p] = reinterpret_cast<const uint4 *>(q)[1];
+  } else {
+    dst[2 * (size_t)i] = reinterpret_cast<const uint4 *>(q)[0];
+    dst[2 * (size_t)i + 1] = reinterpret_cast<const uint4 *>(q)[1];
+  }
 }
 
 // target: ((h_{t+1} - h_t) - r (h_t - h_{t-1})) / s
@@ -416,7 +434,14 @@ static int cnn_loss(Net &n, const Grid3 &g, const float *y, double *loss) {
 static int cnn_pack(Net &n) {
   k_pack_weights<<<(kLayers * kWl + 255) / 256, 256, 0, n.stream>>>(n.w32, n.w16, n.wt16);
   MSG_CHECK_LAUNCH();
-  return MSG_OK;
+  return conv_pack_weights(n.w32, kPl, n.wtc, n.stream);
+}
+
+// Tensor-core forward pass from the plan's input buffer; *out = output channel (N floats).
+static int cnn_forward_tc(Net &n, cudaStream_t s, const float **out) {
+  const float *bias[kLayers];
+  for (int l = 0; l < kLayers; ++l) bias[l] = n.w32 + (size_t)l * kPl + kWl;
+  return conv_forward_tc(n.plan, n.wtc, bias, s, out);
 }
 
 static double host_sumsq_diff(msg_ctx *c, const double *a, const double *b, int *rc) {
@@ -439,27 +464,44 @@ static FeatArgs feat_args(msg_ctx *c, double inv_s, double ratio) {
 
 bool learned_ready(msg_ctx *c) { return c->learned != nullptr; }
 
-// head_new <- h_old + r (h_old - h_old2) + s * CNN(features)
-int learned_guess(msg_ctx *c) {
+// Features of the current state and the tensor-core forward pass (no state change);
+// *s_out / *ratio_out: the increment scale and the dt ratio the features were made with.
+int learned_forward(msg_ctx *c, const float **out, double *s_out, double *ratio_out) {
   Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
   int rc;
   double ss = host_sumsq_diff(c, c->head_old, c->head_old2, &rc);
   if (rc) return rc;
   double s = std::sqrt(ss / c->N) + 1e-30;
   double ratio = c->delt / c->delt_old1;
-  if ((rc = cnn_reserve(n, c->N))) return rc;
-  cudaStream_t saved = n.stream;
-  n.stream = c->stream;
-  Grid3 g{c->nx, c->ny, c->nz, c->nxy, c->N};
-  k_features<<<(c->N + 255) / 256, 256, 0, c->stream>>>(feat_args(c, 1.0 / s, ratio), n.a[0]);
+  if ((rc = conv_plan_get(&n.plan, c->nx, c->ny, c->nz))) return rc;
+  k_features<true><<<(c->N + 255) / 256, 256, 0, c->stream>>>(feat_args(c, 1.0 / s, ratio), conv_plan_input(n.plan),
+                                                               (long long)conv_plan_plane(n.plan));
   MSG_CHECK_LAUNCH();
-  rc = cnn_forward(n, g, n.a[0]);
-  n.stream = saved;
-  if (rc) return rc;
-  k_apply_guess<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->head_new, c->head_old, c->head_old2, ratio, s,
-                                                          n.z[3], n.dead);
-  MSG_CHECK_LAUNCH();
+  if ((rc = cnn_forward_tc(n, c->stream, out))) return rc;
+  if (s_out) *s_out = s;
+  if (ratio_out) *ratio_out = ratio;
   return MSG_OK;
+}
+
+int learned_convs(msg_ctx *c) {
+  Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  const float *o = nullptr;
+  return cnn_forward_tc(n, c->stream, &o);
+}
+
+int learned_check(msg_ctx *c) { return conv_check(reinterpret_cast<msg_cnn *>(c->learned)->net.plan, c->stream); }
+
+// head_new <- h_old + r (h_old - h_old2) + s * CNN(features)
+int learned_guess(msg_ctx *c) {
+  Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  const float *o = nullptr;
+  double s = 0.0, ratio = 0.0;
+  int rc = learned_forward(c, &o, &s, &ratio);
+  if (rc) return rc;
+  k_apply_guess<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->head_new, c->head_old, c->head_old2, ratio, s, o,
+                                                          n.dead);
+  MSG_CHECK_LAUNCH();
+  return conv_check(n.plan, c->stream);
 }
 
 void learned_free(msg_ctx *c) { c->learned = nullptr; }   // the network is owned by its msg_cnn handle
@@ -481,8 +523,11 @@ MSG_API int msg_gpu_cnn_create(int32_t seed, msg_cnn_t **out) {
   MSG_CUDA(cudaMalloc(&n.grad, kNParam * 4));
   MSG_CUDA(cudaMalloc(&n.w16, kLayers * kWl * 2));
   MSG_CUDA(cudaMalloc(&n.wt16, kLayers * kWl * 2));
-  MSG_CUDA(cudaMemset(n.m, 0, kNParam * 4));
-  MSG_CUDA(cudaMemset(n.v, 0, kNParam * 4));
+  MSG_CUDA(cudaMalloc(&n.wtc, kLayers * kWl * 2));
+  // every upload goes through the network's own (non-blocking) stream, so the kernels that
+  // follow on that stream see it
+  MSG_CUDA(cudaMemsetAsync(n.m, 0, kNParam * 4, n.stream));
+  MSG_CUDA(cudaMemsetAsync(n.v, 0, kNParam * 4, n.stream));
   // He-style init on the real fan-in (27 x used input channels); last layer starts at zero
   std::vector<float> w(kNParam, 0.f);
   unsigned long long st = 0x9E3779B97F4A7C15ull ^ (unsigned long long)seed;
@@ -501,7 +546,7 @@ MSG_API int msg_gpu_cnn_create(int32_t seed, msg_cnn_t **out) {
               (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
         }
   }
-  MSG_CUDA(cudaMemcpy(n.w32, w.data(), kNParam * 4, cudaMemcpyHostToDevice));
+  MSG_CUDA(cudaMemcpyAsync(n.w32, w.data(), kNParam * 4, cudaMemcpyHostToDevice, n.stream));
   int rc = cnn_pack(n);
   if (rc) return rc;
   MSG_CUDA(cudaStreamSynchronize(n.stream));
@@ -513,7 +558,8 @@ MSG_API void msg_gpu_cnn_destroy(msg_cnn_t *h) {
   if (!h) return;
   Net &n = h->net;
   cudaStreamSynchronize(n.stream);
-  void *p[] = {n.w32, n.w16, n.wt16, n.m, n.v, n.grad, n.part, n.dz, n.dz2, n.loss_part};
+  void *p[] = {n.w32, n.w16, n.wt16, n.wtc, n.m, n.v, n.grad, n.part, n.dz, n.dz2, n.loss_part};
+  conv_plan_free(n.plan);
   for (void *q : p) if (q) cudaFree(q);
   for (int l = 0; l < kLayers; ++l) { if (n.a[l]) cudaFree(n.a[l]); if (n.z[l]) cudaFree(n.z[l]); }
   for (auto &smp : n.data) { cudaFree(smp.x); cudaFree(smp.y); }
@@ -538,7 +584,7 @@ MSG_API int msg_gpu_cnn_get_weights(msg_cnn_t *h, float *w) {
 
 MSG_API int msg_gpu_cnn_set_weights(msg_cnn_t *h, const float *w) {
   if (!h || !w) return MSG_ERR_ARG;
-  MSG_CUDA(cudaMemcpy(h->net.w32, w, kNParam * 4, cudaMemcpyHostToDevice));
+  MSG_CUDA(cudaMemcpyAsync(h->net.w32, w, kNParam * 4, cudaMemcpyHostToDevice, h->net.stream));
   int rc = cnn_pack(h->net);
   if (rc) return rc;
   MSG_CUDA(cudaStreamSynchronize(h->net.stream));
@@ -560,7 +606,7 @@ MSG_API int msg_gpu_cnn_collect(msg_cnn_t *h, msg_ctx_t *c) {
   smp.g = Grid3{c->nx, c->ny, c->nz, c->nxy, c->N};
   MSG_CUDA(cudaMalloc(&smp.x, (size_t)c->N * kC * 2));
   MSG_CUDA(cudaMalloc(&smp.y, (size_t)c->N * 4));
-  k_features<<<(c->N + 255) / 256, 256, 0, c->stream>>>(feat_args(c, 1.0 / s, ratio), smp.x);
+  k_features<false><<<(c->N + 255) / 256, 256, 0, c->stream>>>(feat_args(c, 1.0 / s, ratio), smp.x, 0);
   MSG_CHECK_LAUNCH();
   k_target<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->head_new, c->head_old, c->head_old2, ratio, 1.0 / s,
                                                      smp.y);
@@ -582,8 +628,9 @@ MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *h, int32_t nx, int32_t ny, int32_t
   for (size_t k = 0; k < N * kC; ++k) xb[k] = __float2bfloat16(x[k]);
   MSG_CUDA(cudaMalloc(&smp.x, N * kC * 2));
   MSG_CUDA(cudaMalloc(&smp.y, N * 4));
-  MSG_CUDA(cudaMemcpy(smp.x, xb.data(), N * kC * 2, cudaMemcpyHostToDevice));
-  MSG_CUDA(cudaMemcpy(smp.y, y, N * 4, cudaMemcpyHostToDevice));
+  MSG_CUDA(cudaMemcpyAsync(smp.x, xb.data(), N * kC * 2, cudaMemcpyHostToDevice, h->net.stream));
+  MSG_CUDA(cudaMemcpyAsync(smp.y, y, N * 4, cudaMemcpyHostToDevice, h->net.stream));
+  MSG_CUDA(cudaStreamSynchronize(h->net.stream));
   h->net.data.push_back(smp);
   return MSG_OK;
 }
@@ -608,6 +655,21 @@ MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *h, int32_t sample, double *loss, fl
     MSG_CUDA(cudaStreamSynchronize(n.stream));
     MSG_CUDA(cudaMemcpy(out, n.z[3], (size_t)smp.g.N * 4, cudaMemcpyDeviceToHost));
   }
+  return MSG_OK;
+}
+
+// Inference pass of the tensor-core path on one stored sample: out = N floats.
+MSG_API int msg_gpu_cnn_infer(msg_cnn_t *h, int32_t sample, float *out) {
+  if (!h || !out || sample < 0 || sample >= (int)h->net.data.size()) return MSG_ERR_ARG;
+  Net &n = h->net;
+  Sample &smp = n.data[sample];
+  int rc;
+  if ((rc = conv_plan_get(&n.plan, smp.g.nx, smp.g.ny, smp.g.nz))) return rc;
+  if ((rc = conv_plan_load_compact(n.plan, smp.x, n.stream))) return rc;
+  const float *o = nullptr;
+  if ((rc = cnn_forward_tc(n, n.stream, &o))) return rc;
+  if ((rc = conv_check(n.plan, n.stream))) return rc;
+  MSG_CUDA(cudaMemcpy(out, o, (size_t)smp.g.N * 4, cudaMemcpyDeviceToHost));
   return MSG_OK;
 }
 

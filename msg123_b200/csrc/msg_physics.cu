@@ -192,12 +192,28 @@ struct CellArgs {
   double *srat, *kr, *kr_per, *sto, *stod;
 };
 
-template <bool ASM>
+// ASM = false: calc_func's pass; ASM = true: make_matvec's pass.  REUSE (with ASM): S, kr
+// and the storage term at h are already in srat / kr / sto from a residual evaluation at
+// the same h (the previous Newton iteration ends with one), so only the perturbed
+// evaluation at h + newper is made -- the same values bit for bit, half the pow calls.
+template <bool ASM, bool REUSE = false>
 __global__ void k_cell(int N, CellArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double hi = a.h[i], top = a.top[i];
   float reta = a.reta[i], retn = a.retn[i], resi = a.resi[i], poro = a.poro[i], ss = a.ss[i];
+  if (REUSE) {
+    VG v;
+    v.S = a.srat[i];
+    v.alp = (__dsub_rn(hi, top) < 0.0) ? 0.0 : (double)ss;   // vg_eval's branch at pertur = 0
+    VG w = vg_eval(hi, top, a.newper, reta, retn, resi, poro, ss);
+    a.kr_per[i] = w.kr;
+    double deri_srat = __dmul_rn(__dsub_rn(w.S, v.S), a.newper_inv);
+    double deri_stor = __dmul_rn(__dmul_rn(v.alp, deri_srat), hi);
+    double x = __dadd_rn(__dadd_rn(__dmul_rn((double)poro, deri_srat), __dmul_rn(v.alp, v.S)), deri_stor);
+    a.stod[i] = __dmul_rn(__dmul_rn(-x, a.delt_inv), a.vol[i]);
+    return;
+  }
   VG v = vg_eval(hi, top, 0.0, reta, retn, resi, poro, ss);
   double vol = a.vol[i];
   double ch1 = __dmul_rn(__dmul_rn(v.alp, a.s_old[i]), a.h_old[i]);
@@ -268,8 +284,7 @@ __device__ __forceinline__ double surf_term(double infs, double insh, double top
 }
 
 template <bool ASM>
-__global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
-  __shared__ double sh[8];
+__device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
   const Geo g = a.g;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double f2 = 0.0;
@@ -363,6 +378,19 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
     double s = block_sum<256>(f2, sh);
     if (threadIdx.x == 0) a.part[blockIdx.x] = s;
   }
+}
+
+// Residual pass: at most 48 registers so that five 256-thread blocks stay resident per SM
+// (the pass is bound by the latency of its 27 loads per cell, not by bandwidth).
+__global__ void __launch_bounds__(256, 5) k_flux_res(FluxArgs a) {
+  __shared__ double sh[8];
+  flux_body<false>(a, sh);
+}
+
+// Assembly pass (residual + Jacobian rows).
+__global__ void __launch_bounds__(256) k_flux_asm(FluxArgs a) {
+  __shared__ double sh[8];
+  flux_body<true>(a, sh);
 }
 
 // DIA -> reference CSR order export of lumat.
@@ -521,14 +549,15 @@ int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
   FluxArgs a = flux_args(c, h);
   a.F = F;
   a.part = norm ? c->part : nullptr;
-  k_flux<false><<<nblk(c->N), 256, 0, c->stream>>>(a);
+  k_flux_res<<<nblk(c->N), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
 
-int launch_make_matvec(msg_ctx *c) {
+int launch_make_matvec(msg_ctx *c, bool reuse) {
   const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
-  k_cell<true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
+  if (reuse) k_cell<true, true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
+  else k_cell<true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, c->head_new);
   a.F = c->rhs;
@@ -537,7 +566,7 @@ int launch_make_matvec(msg_ctx *c) {
   a.dmat_f = c->dmat_f;
   a.lu_f = c->lu_f;
   a.part = c->part;
-  k_flux<true><<<nblk(c->N), 256, 0, c->stream>>>(a);
+  k_flux_asm<<<nblk(c->N), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }

@@ -33,6 +33,7 @@ def _lib():
         L.msg_gpu_cnn_nsamples.argtypes = [vp]
         L.msg_gpu_cnn_add_sample.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, abi.PF, abi.PF]
         L.msg_gpu_cnn_loss_grad.argtypes = [vp, C.c_int32, abi.PD, abi.PF, abi.PF]
+        L.msg_gpu_cnn_infer.argtypes = [vp, C.c_int32, abi.PF]
         L.msg_gpu_cnn_train.argtypes = [vp, C.c_int32, C.c_float, C.c_float, C.c_int32, abi.PD]
         L.msg_gpu_cnn_attach.argtypes = [vp, vp]
         L.msg_gpu_guess_fallbacks.argtypes = [vp]
@@ -92,6 +93,12 @@ class Cnn:
         _check(_lib().msg_gpu_cnn_loss_grad(self.h, int(sample), C.byref(loss), abi.fptr(g), abi.fptr(o)),
                "cnn_loss_grad")
         return loss.value, g, o
+
+    def infer(self, sample, n):
+        """Output of the tensor-core (tcgen05) inference path on stored sample `sample`."""
+        o = np.zeros(n, np.float32)
+        _check(_lib().msg_gpu_cnn_infer(self.h, int(sample), abi.fptr(o)), "cnn_infer")
+        return o
 
     def train(self, iters, lr=1e-3, weight_decay=1e-4, seed=0):
         loss = C.c_double()

@@ -59,6 +59,30 @@ def test_cnn_gradients_against_reference(shape):
         assert relerr(gb, rb) < 3e-2, l
 
 
+@pytest.mark.parametrize("shape", [(10, 9, 7), (33, 5, 6), (130, 4, 3), (256, 6, 5)])
+def test_tensor_core_inference_against_reference(shape):
+    """The tcgen05 inference path (TMA halo tiles of 128 cells, TMEM accumulators) against
+    the float64 reference and against the mma.sync training forward.  Shapes cover a row
+    shorter than one tile, a partial second tile and whole tiles."""
+    from msg123_b200.learned import Cnn
+    rng = np.random.default_rng(7)
+    nx, ny, nz = shape
+    x = np.zeros((nz, ny, nx, 16), np.float32)
+    x[..., :7] = rng.standard_normal((nz, ny, nx, 7))
+    y = np.zeros((nz, ny, nx), np.float32)
+    layers = _rand_layers(rng)
+    cnn = Cnn(seed=3)
+    cnn.set_weights(_flat(layers))
+    cnn.add_sample(shape, x.reshape(-1, 16), y.reshape(-1))
+    out_tc = cnn.infer(0, nx * ny * nz)
+    _, _, out_mma = cnn.loss_grad(0, want_grad=False, want_out=True, n=nx * ny * nz)
+    _, out_r, _ = cnn_ref.loss_and_grad(layers, x, y)
+    assert np.all(np.isfinite(out_tc))
+    assert relerr(out_tc, out_r.reshape(-1)) < 3e-2
+    assert relerr(out_tc, out_mma) < 1e-2
+    cnn.close()
+
+
 def test_training_lowers_loss():
     from msg123_b200.learned import Cnn, generate
     kw = dict(amg_lag=1, precision=1)
