@@ -36,6 +36,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-timesteps/s at 1e-8 rel head tol"
+# DRAM bytes per cell of one calc_func (k_cell<false> + k_flux_res), from one ncu capture of
+# the 256x256x64 block (dram__bytes_read.sum + dram__bytes_write.sum, both kernels) divided
+# by its 4,194,304 cells; traffic grows in proportion to the cells.
+TRAFFIC_CALC_FUNC_PER_CELL = 150.0
+TRAFFIC_SOURCE = "profiles/calc_func_kernels_hetero_256x256x64.md, scaled by cells"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 # Algorithmic bytes per cell of the kernels timed by msg_gpu_kernel_time (compulsory
@@ -47,8 +52,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 #                    sto, stod) 100 + assembly pass (h, kr, kr_per, hy, ab, sto, stod ->
 #                    rhs, dmat, six lu, FP32 images 28) 180
 ALG_BYTES = {0: 72.0, 1: 164.0, 2: 280.0}
-KERNEL_NAMES = {0: "stencil SpMV (FP64, DIA)", 1: "calc_func (vG + flux)",
+KERNEL_NAMES = {0: "stencil SpMV (FP64, DIA)", 1: "calc_func (vG pass + flux pass)",
                 2: "make_matvec (vG pair + Jacobian assembly)"}
+# Learned-guess CNN on the tensor cores: 4 convolutions x 27 taps x 16 x 16 (channels padded
+# to 16, as the tcgen05 MMA computes them) x 2 flops per cell.
+CNN_FLOP_PER_CELL = 4 * 27 * 16 * 16 * 2
 
 
 def load_peaks():
@@ -126,10 +134,12 @@ def barrier(dist):
 
 
 def reduce(dist, v, op):
+    """MAX or SUM of a host scalar over the ranks (NCCL on the GPUs; gloo in the CPU tests)."""
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -251,30 +261,38 @@ def main():
     # kernel timings for the roofline (state of the last timed step, library stream)
     peaks, src = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    tc_peak = float(peaks.get("bf16_tflops", 1590.0))
     kt = {w: g.kernel_time(w, reps=10) for w in (0, 1, 2)}
     gbs = {w: ALG_BYTES[w] * prob.ncalc / (kt[w] * 1e-3) / 1e9 for w in kt}
     t_prec = g.kernel_time(3, reps=5)
     t_setup = g.kernel_time(4, reps=2)
+    t_cnn = g.kernel_time(5, reps=5)
+    cnn_tflops = CNN_FLOP_PER_CELL * prob.ncalc / (t_cnn * 1e-3) / 1e12
 
     # end to end through the public API, state in host memory
     e2e = None
     if not args.no_e2e:
-        s = g.get_state()
-        h_new, h_old, s_old, surf = s["head_new"], s["head_old"], s["srat_old"], s["surf_head"]
+        import torch
         N, S = prob.ncalc, prob.ncals
+        # state in pinned host memory, copied in and out through the public C ABI every step
+        pin = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+               for k, n in (("head_new", N), ("head_old", N), ("srat_new", N), ("srat_old", N), ("surf_head", S))}
+        g.get_state(out=pin)
         barrier(dist)
         t0 = time.perf_counter()
         acc = 0
         for _ in range(args.steps):
-            g.set_state(head_new=h_new, head_old=h_old, srat_old=s_old, surf_head=surf)
+            g.set_state(head_new=pin["head_new"], head_old=pin["head_old"], srat_old=pin["srat_old"],
+                        surf_head=pin["surf_head"])
             rc2, st2 = g.advance(nsteps=1)
-            s2 = g.get_state()
-            h_new, h_old, s_old, surf = s2["head_new"], s2["head_old"], s2["srat_new"], s2["surf_head"]
+            g.get_state(out=pin)
+            pin["srat_old"][:] = pin["srat_new"]
             acc += st2["accepted"]
         te = reduce(dist, time.perf_counter() - t0, "max")
         e2e = {"value": reduce(dist, float(prob.ncalc * acc), "sum") / te, "unit": "cell-timesteps/s",
-               "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 5 * N * 8 + S * 8,
-               "path": "mixed + learned through msg_gpu_set_state / msg_gpu_advance / msg_gpu_get_state"}
+               "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 4 * N * 8 + S * 8,
+               "path": "mixed + learned through msg_gpu_set_state / msg_gpu_advance / msg_gpu_get_state, "
+                       "pinned host buffers"}
     g.close()
 
     # ---- plain FP64 reference method on the same field ----------------------------------
@@ -313,12 +331,16 @@ def main():
                        "krylov_per_step": st["krylov_total"] / max(st["accepted"], 1),
                        "backtracks": st["back_total"], "simulated_s": st["current_t"]},
             "plain_fp64": plain,
-            "roofline": {"kernel": KERNEL_NAMES[2], "bound": "hbm", "achieved": gbs[2], "peak": hbm,
-                         "unit": "GB/s", "frac": gbs[2] / hbm, "peak_source": src,
-                         "alg_bytes_per_cell": ALG_BYTES[2], "cells_per_launch": prob.ncalc,
-                         "ms_per_launch": kt[2], "traffic": None,
-                         "others": {KERNEL_NAMES[w]: {"ms": kt[w], "GB/s": gbs[w], "frac": gbs[w] / hbm}
-                                    for w in (0, 1)},
+            "roofline": {"kernel": KERNEL_NAMES[1], "bound": "hbm", "achieved": gbs[1], "peak": hbm,
+                         "unit": "GB/s", "frac": gbs[1] / hbm, "peak_source": src,
+                         "alg_bytes_per_cell": ALG_BYTES[1], "cells_per_launch": prob.ncalc,
+                         "ms_per_launch": kt[1], "traffic": TRAFFIC_CALC_FUNC_PER_CELL * prob.ncalc,
+                         "traffic_source": TRAFFIC_SOURCE,
+                         "others": dict({KERNEL_NAMES[w]: {"ms": kt[w], "GB/s": gbs[w], "frac": gbs[w] / hbm}
+                                         for w in (0, 2)},
+                                        **{"learned-guess CNN, 4 tcgen05 convolutions": {
+                                            "ms": t_cnn, "TFLOP/s": cnn_tflops, "frac": cnn_tflops / tc_peak,
+                                            "bound": "tensor", "peak_TFLOP/s": tc_peak}}),
                          "vcycle_mixed_ms": t_prec, "amg_setup_ms": t_setup},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }

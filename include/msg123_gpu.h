@@ -192,6 +192,13 @@ MSG_API int msg_gpu_advance(msg_ctx_t *ctx, int32_t nsteps, double rech_until, d
  * storage, flow, recharge, well, surface, river, lake, sea (+ out[8] drainage),
  * each a volume over the step (rate * delt). */
 MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
+/* Restart file in the reference's format (replaces write_rest, Nonlinear_solution.f90:792-816,
+   and write_out_restf, Write_output.f90:415-432): gfortran sequential unformatted records
+   [real(DP) time][head_new * len_scal, ncalc values], 4-byte length markers. */
+MSG_API int msg_gpu_write_restart(msg_ctx_t *ctx, const char *path);
+/* Reads such a file (replaces the restart branch of assign_initv, Assign_calculation.f90:416-434):
+   head = value * (1 / len_scal); host code only, no GPU needed. */
+MSG_API int msg_gpu_read_restart(const char *path, int32_t ncalc, double len_scal, double *head, double *time);
 
 /* Device time spent in the last advance/numsol call split by phase (ms):
  * [0] assembly, [1] Krylov, [2] AMG setup, [3] residual evaluations, [4] total. */
@@ -249,6 +256,11 @@ MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *cnn, int32_t nx, int32_t ny, int32
 /* inference pass of the tensor-core (tcgen05) path on a stored sample; out: N floats.
    No reference counterpart (the learned guess is an addition of this library). */
 MSG_API int msg_gpu_cnn_infer(msg_cnn_t *cnn, int32_t sample, float *out);
+/* test hook for the bounded waits: as msg_gpu_cnn_infer, but the first convolution never
+   loads the input box of tile `tile`; the kernel's wait on it runs out (about 1 s), the
+   pass ends normally and the call returns MSG_ERR_CUDA with the wait's code in
+   msg_gpu_last_error().  No reference counterpart. */
+MSG_API int msg_gpu_cnn_infer_withhold(msg_cnn_t *cnn, int32_t sample, int32_t tile, float *out);
 /* mean squared error on one sample; grad (msg_gpu_cnn_nparam floats) and out (N) may be NULL */
 MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *cnn, int32_t sample, double *loss, float *grad, float *out);
 /* AdamW training over the stored samples */

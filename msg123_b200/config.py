@@ -210,12 +210,19 @@ def make_hetero(shape=(256, 256, 64), d=(1.0, 1.0, 0.25), seed=2024, sigma=1.0, 
     return p
 
 
-def make_member(seed, **pkw):
-    """Ensemble member: nx, ny ~ U{64..160}, nz ~ U{32..48}, sigma_lnK ~ U[0.5, 1.5]."""
+def member_draw(seed):
+    """Shape and lnKs spread of ensemble member `seed` (no fields built):
+    nx, ny ~ U{64..160}, nz ~ U{32..48}, sigma_lnK ~ U[0.5, 1.5]."""
     rng = np.random.default_rng(10_000 + seed)
     nx = int(rng.integers(64, 161)); ny = int(rng.integers(64, 161)); nz = int(rng.integers(32, 49))
     sigma = float(rng.uniform(0.5, 1.5))
-    return make_hetero(shape=(nx, ny, nz), seed=seed, sigma=sigma, precision=1, **pkw)
+    return (nx, ny, nz), sigma
+
+
+def make_member(seed, **pkw):
+    """Ensemble member `seed` (member_draw) on the config-2 generator, mixed precision."""
+    shape, sigma = member_draw(seed)
+    return make_hetero(shape=shape, seed=seed, sigma=sigma, precision=1, **pkw)
 
 
 def make_config(name, **kw):

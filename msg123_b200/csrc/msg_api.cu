@@ -10,6 +10,8 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
+#include <cstdio>
+#include <vector>
 #include <atomic>
 #include <new>
 #include <string>
@@ -771,6 +773,56 @@ int msg_gpu_advance(msg_ctx_t *c, int32_t nsteps, double rech_until, double rech
   cudaEventElapsedTime(&tot, c->ev[5], c->ev[6]);
   c->t_ms[4] = tot;
   return rc;
+}
+
+// ---- restart file (checkpoint / resume) ------------------------------------------------
+// The reference's restart file (write_rest, Nonlinear_solution.f90:792-816, and
+// write_out_restf, Write_output.f90:415-432): gfortran sequential unformatted, two records
+// -- real(DP) time, then head_new * len_scal for the ncalc cells -- each framed by a 4-byte
+// record length before and after.  Records of 2^31 bytes or more (gfortran subrecords)
+// are rejected.
+static bool put_record(FILE *f, const void *p, size_t bytes) {
+  const int32_t m = (int32_t)bytes;
+  return fwrite(&m, 4, 1, f) == 1 && fwrite(p, 1, bytes, f) == bytes && fwrite(&m, 4, 1, f) == 1;
+}
+
+static bool get_record(FILE *f, void *p, size_t bytes) {
+  int32_t m0 = 0, m1 = 0;
+  return fread(&m0, 4, 1, f) == 1 && (size_t)m0 == bytes && fread(p, 1, bytes, f) == bytes &&
+         fread(&m1, 4, 1, f) == 1 && m1 == m0;
+}
+
+int msg_gpu_write_restart(msg_ctx_t *c, const char *path) {
+  if (!c || !path) return MSG_ERR_ARG;
+  const size_t N = c->N;
+  if (N * 8 > 0x7fffffffull) { set_error("write_restart: record of %zu bytes needs subrecords", N * 8); return MSG_ERR_SIZE; }
+  std::vector<double> h(N);
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  MSG_CUDA(cudaMemcpy(h.data(), c->head_new, N * 8, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < N; ++i) h[i] = h[i] * c->len_scal;
+  const double t = c->current_t;   // already rounded to real(SP), as now_time is
+  FILE *f = fopen(path, "wb");
+  if (!f) { set_error("write_restart: cannot open %s", path); return MSG_ERR_ARG; }
+  const bool ok = put_record(f, &t, 8) && put_record(f, h.data(), N * 8);
+  if (fclose(f) != 0 || !ok) { set_error("write_restart: write failed on %s", path); return MSG_ERR_ARG; }
+  return MSG_OK;
+}
+
+// assign_initv with a restart file (Assign_calculation.f90:416-434): time from record 1,
+// heads = record 2 * (1 / len_scal).
+int msg_gpu_read_restart(const char *path, int32_t ncalc, double len_scal, double *head, double *time) {
+  if (!path || ncalc < 1 || !head || !(len_scal > 0.0)) return MSG_ERR_ARG;
+  if ((size_t)ncalc * 8 > 0x7fffffffull) { set_error("read_restart: record needs subrecords"); return MSG_ERR_SIZE; }
+  FILE *f = fopen(path, "rb");
+  if (!f) { set_error("read_restart: cannot open %s", path); return MSG_ERR_ARG; }
+  double t = 0.0;
+  const bool ok = get_record(f, &t, 8) && get_record(f, head, (size_t)ncalc * 8);
+  fclose(f);
+  if (!ok) { set_error("read_restart: %s is not a restart file of %d cells", path, ncalc); return MSG_ERR_SIZE; }
+  const double inv = 1.0 / len_scal;
+  for (int32_t i = 0; i < ncalc; ++i) head[i] = head[i] * inv;
+  if (time) *time = t;
+  return MSG_OK;
 }
 
 int msg_gpu_calc_mass(msg_ctx_t *c, double *out9) {

@@ -75,6 +75,7 @@ struct TcArgs {
   __nv_bfloat16 *act_out;    // hidden layer output (padded, chunk-planar)
   float *out;                // output layer: channel 0, interior order
   int *err;
+  int withhold;              // test hook: the box of this tile is never loaded (-1: none)
 };
 
 // ---------------------------------------------------------------------------------
@@ -226,13 +227,17 @@ __global__ void __launch_bounds__(kThreadsTC, kCtaPerSm) k_conv_tc(const __grid_
   if (warp == 0) {
     if (lane == 0) {
       // ---- TMA producer ----
-      int j = 0;
+      int j = 0, withheld = -1;
       for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++j) {
         const int s = j % kStages;
         if (!mbar_wait(cb + 32 + 8 * s, ((j / kStages) & 1) ^ 1, abort_flag)) {
           atomicCAS(a.err, 0, 1);
           *abort_flag = 1;
           break;
+        }
+        if (t == a.withhold) {   // the consumer's bounded wait on this stage runs out
+          withheld = j;
+          continue;
         }
         const int tx = t % a.ntx, r = t / a.ntx, ty = r % a.nty, z = r / a.nty;
         mbar_expect_tx(cb + 8 * s, kBoxBytes);
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kThreadsTC, kCtaPerSm) k_conv_tc(const __grid_
       }
       // every issued box must have landed before the CTA may exit
       for (int q = (j > kStages ? j - kStages : 0); q < j; ++q)
-        if (!mbar_wait(cb + 8 * (q % kStages), (q / kStages) & 1, nullptr)) atomicCAS(a.err, 0, 5);
+        if (q != withheld && !mbar_wait(cb + 8 * (q % kStages), (q / kStages) & 1, nullptr)) atomicCAS(a.err, 0, 5);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -442,8 +447,9 @@ int conv_pack_weights(const float *w32, int layer_stride, __nv_bfloat16 *wpk, cu
 }
 
 int conv_forward_tc(ConvPlan *p, const __nv_bfloat16 *wpk, const float *const bias[4], cudaStream_t s,
-                    const float **out) {
+                    const float **out, int withhold) {
   TcArgs a;
+  a.withhold = withhold;
   a.nx = p->nx; a.ny = p->ny; a.px = p->px; a.py = p->py;
   a.ntx = (p->nx + kTX - 1) / kTX;
   a.nty = (p->ny + kTY - 1) / kTY;
@@ -463,6 +469,7 @@ int conv_forward_tc(ConvPlan *p, const __nv_bfloat16 *wpk, const float *const bi
       a.act_out = p->buf[nxt];
       k_conv_tc<0><<<grid, kThreadsTC, kSmemTC, s>>>(p->map[in], a);
       MSG_CHECK_LAUNCH();
+      a.withhold = -1;
       in = nxt;
       nxt = (nxt == 1) ? 2 : 1;
     } else {
@@ -480,7 +487,8 @@ int conv_forward_tc(ConvPlan *p, const __nv_bfloat16 *wpk, const float *const bi
 int conv_check(ConvPlan *p, cudaStream_t s) {
   MSG_CUDA(cudaStreamSynchronize(s));
   if (*p->err_host) {
-    set_error("tensor-core convolution: a wait ran out (code %d)", *p->err_host);
+    set_error("tensor-core convolution: a bounded wait ran out (code %d: 1 producer, 2 MMA issuer, 3 epilogue, "
+              "5 copy drain, 6 MMA drain)", *p->err_host);
     return MSG_ERR_CUDA;
   }
   return MSG_OK;

@@ -26,8 +26,10 @@ int conv_plan_load_compact(ConvPlan *plan, const __nv_bfloat16 *x, cudaStream_t 
 // wpk: weights packed for the tensor cores, [layer][tap][k chunk][co][8 ci] bf16
 // (512 B per tap); bias: bias[l] points at 16 floats of layer l.  *out receives
 // the output channel in interior order (N floats, owned by the plan).
+// withhold >= 0 (tests only): the first layer never loads the box of that tile, so the
+// consumer's bounded wait runs out and the pass reports an error instead of hanging.
 int conv_forward_tc(ConvPlan *plan, const __nv_bfloat16 *wpk, const float *const bias[4], cudaStream_t s,
-                    const float **out);
+                    const float **out, int withhold = -1);
 // Synchronise the stream and report a wait that ran out inside the last forward pass.
 int conv_check(ConvPlan *plan, cudaStream_t s);
 

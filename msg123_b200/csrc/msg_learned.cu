@@ -438,10 +438,10 @@ static int cnn_pack(Net &n) {
 }
 
 // Tensor-core forward pass from the plan's input buffer; *out = output channel (N floats).
-static int cnn_forward_tc(Net &n, cudaStream_t s, const float **out) {
+static int cnn_forward_tc(Net &n, cudaStream_t s, const float **out, int withhold = -1) {
   const float *bias[kLayers];
   for (int l = 0; l < kLayers; ++l) bias[l] = n.w32 + (size_t)l * kPl + kWl;
-  return conv_forward_tc(n.plan, n.wtc, bias, s, out);
+  return conv_forward_tc(n.plan, n.wtc, bias, s, out, withhold);
 }
 
 static double host_sumsq_diff(msg_ctx *c, const double *a, const double *b, int *rc) {
@@ -659,7 +659,7 @@ MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *h, int32_t sample, double *loss, fl
 }
 
 // Inference pass of the tensor-core path on one stored sample: out = N floats.
-MSG_API int msg_gpu_cnn_infer(msg_cnn_t *h, int32_t sample, float *out) {
+static int cnn_infer(msg_cnn_t *h, int32_t sample, float *out, int withhold) {
   if (!h || !out || sample < 0 || sample >= (int)h->net.data.size()) return MSG_ERR_ARG;
   Net &n = h->net;
   Sample &smp = n.data[sample];
@@ -667,10 +667,17 @@ MSG_API int msg_gpu_cnn_infer(msg_cnn_t *h, int32_t sample, float *out) {
   if ((rc = conv_plan_get(&n.plan, smp.g.nx, smp.g.ny, smp.g.nz))) return rc;
   if ((rc = conv_plan_load_compact(n.plan, smp.x, n.stream))) return rc;
   const float *o = nullptr;
-  if ((rc = cnn_forward_tc(n, n.stream, &o))) return rc;
+  if ((rc = cnn_forward_tc(n, n.stream, &o, withhold))) return rc;
   if ((rc = conv_check(n.plan, n.stream))) return rc;
   MSG_CUDA(cudaMemcpy(out, o, (size_t)smp.g.N * 4, cudaMemcpyDeviceToHost));
   return MSG_OK;
+}
+
+MSG_API int msg_gpu_cnn_infer(msg_cnn_t *h, int32_t sample, float *out) { return cnn_infer(h, sample, out, -1); }
+
+MSG_API int msg_gpu_cnn_infer_withhold(msg_cnn_t *h, int32_t sample, int32_t tile, float *out) {
+  if (tile < 0) return MSG_ERR_ARG;
+  return cnn_infer(h, sample, out, tile);
 }
 
 // `iters` AdamW steps over the stored samples (sample order from `seed`); returns the

@@ -30,12 +30,15 @@ def _lib():
 
 
 class Ensemble:
-    def __init__(self, nmembers=64, seed0=0, **overrides):
+    def __init__(self, nmembers=64, seed0=0, seeds=None, **overrides):
+        """Members seed0 .. seed0 + nmembers - 1, or the explicit member `seeds` (a rank's share)."""
         kw = dict(ENSEMBLE)
         kw.update(overrides)
+        self.seeds = list(seeds) if seeds is not None else [seed0 + k for k in range(nmembers)]
+        nmembers = len(self.seeds)
         self.members = []
-        for k in range(nmembers):
-            p = make_member(seed0 + k)
+        for k in self.seeds:
+            p = make_member(k)
             g = GpuSolver(p, **kw)
             p.dis2face = p.face_area = None      # only needed while the context is created
             self.members.append(g)

@@ -34,6 +34,7 @@ def _lib():
         L.msg_gpu_cnn_add_sample.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, abi.PF, abi.PF]
         L.msg_gpu_cnn_loss_grad.argtypes = [vp, C.c_int32, abi.PD, abi.PF, abi.PF]
         L.msg_gpu_cnn_infer.argtypes = [vp, C.c_int32, abi.PF]
+        L.msg_gpu_cnn_infer_withhold.argtypes = [vp, C.c_int32, C.c_int32, abi.PF]
         L.msg_gpu_cnn_train.argtypes = [vp, C.c_int32, C.c_float, C.c_float, C.c_int32, abi.PD]
         L.msg_gpu_cnn_attach.argtypes = [vp, vp]
         L.msg_gpu_guess_fallbacks.argtypes = [vp]
@@ -99,6 +100,13 @@ class Cnn:
         o = np.zeros(n, np.float32)
         _check(_lib().msg_gpu_cnn_infer(self.h, int(sample), abi.fptr(o)), "cnn_infer")
         return o
+
+    def infer_withhold(self, sample, n, tile):
+        """Test hook: inference with the input box of `tile` never loaded.  Returns the
+        library status (MSG_ERR_CUDA expected) and the error message."""
+        o = np.zeros(n, np.float32)
+        rc = _lib().msg_gpu_cnn_infer_withhold(self.h, int(sample), int(tile), abi.fptr(o))
+        return rc, load_library().msg_gpu_last_error().decode()
 
     def train(self, iters, lr=1e-3, weight_decay=1e-4, seed=0):
         loss = C.c_double()

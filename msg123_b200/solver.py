@@ -86,6 +86,17 @@ def dense_inverse(a):
     return inv
 
 
+def read_restart(path, ncalc, len_scal):
+    """(heads, time) from a restart file of the reference (host code, no GPU)."""
+    L = load_library()
+    L.msg_gpu_read_restart.argtypes = [C.c_char_p, C.c_int32, C.c_double, abi.PD, abi.PD]
+    h = np.zeros(int(ncalc))
+    t = np.zeros(1)
+    _check(L.msg_gpu_read_restart(os.fsencode(path), int(ncalc), C.c_double(len_scal), dptr(h), dptr(t)),
+           "read_restart")
+    return h, float(t[0])
+
+
 def _check(rc, what):
     if rc < 0:
         msg = load_library().msg_gpu_last_error().decode(errors="replace")
@@ -157,14 +168,39 @@ class GpuSolver:
         arrs = [None if a is None else _f64(a) for a in (head_new, head_old, srat_old, surf_head)]
         _check(load_library().msg_gpu_set_state(self.h, *(dptr(a) for a in arrs), C.c_double(delt)), "set_state")
 
-    def get_state(self):
+    def get_state(self, out=None):
+        """Copy the state to host arrays (new float64 arrays, or the C-contiguous float64
+        arrays of `out`, e.g. views of pinned memory)."""
         N, S = self.n, self.ncals
-        out = dict(head_new=np.zeros(N), head_old=np.zeros(N), srat_new=np.zeros(N), srat_old=np.zeros(N),
-                   surf_head=np.zeros(S))
+        if out is None:
+            out = dict(head_new=np.zeros(N), head_old=np.zeros(N), srat_new=np.zeros(N), srat_old=np.zeros(N),
+                       surf_head=np.zeros(S))
+        for k, n in (("head_new", N), ("head_old", N), ("srat_new", N), ("srat_old", N), ("surf_head", S)):
+            a = out[k]
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n:
+                raise ValueError(f"get_state: {k} must be a C-contiguous float64 array of {n}")
         _check(load_library().msg_gpu_get_state(self.h, *(dptr(out[k]) for k in
                                                          ("head_new", "head_old", "srat_new", "srat_old",
                                                           "surf_head"))), "get_state")
         return out
+
+    def guess_fallbacks(self):
+        """Learned guesses whose Newton run failed and was redone from the extrapolation."""
+        L = load_library()
+        L.msg_gpu_guess_fallbacks.argtypes = [C.c_void_p]
+        return int(L.msg_gpu_guess_fallbacks(self.h))
+
+    def guess_rejected(self):
+        """Learned guesses not used because their residual exceeded the extrapolation's."""
+        L = load_library()
+        L.msg_gpu_guess_rejected.argtypes = [C.c_void_p]
+        return int(L.msg_gpu_guess_rejected(self.h))
+
+    def write_restart(self, path):
+        """Restart file of the reference (gfortran records: time, head * len_scal)."""
+        L = load_library()
+        L.msg_gpu_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+        _check(L.msg_gpu_write_restart(self.h, os.fsencode(path)), "write_restart")
 
     def set_recharge(self, rech):
         _check(load_library().msg_gpu_set_recharge(self.h, dptr(_f64(rech))), "set_recharge")
