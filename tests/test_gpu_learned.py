@@ -114,4 +114,5 @@ def test_learned_guess_newton_gain(shape, seed):
           f"(fallbacks, rejected {fb})")
     assert s2["accepted"] == 12
     assert n1 < n0
-    assert n2 <= n1 * 1.1
+    assert n2 < n0                 # gain over the reference's start from the previous head
+    assert n2 <= n1 * 1.1          # and no loss against the plain extrapolation
