@@ -16,8 +16,8 @@
 // (27 x tcgen05.mma M128 N16 K16, BF16 inputs), alternating between kChains accumulators
 // (summed in the epilogue) so that successive MMAs do not wait on one accumulator.
 //
-// Warp roles (192 threads, two persistent CTAs per SM, 83 KB of shared memory each):
-//   warp 0      TMA producer over a 4-stage ring; allocates and frees the TMEM columns
+// Warp roles (192 threads, three persistent CTAs per SM, 67 KB of shared memory each):
+//   warp 0      TMA producer over a 3-stage ring; allocates and frees the TMEM columns
 //   warp 1      MMA issuer (one thread); commits each tile to the stage's "empty" barrier
 //               and to the accumulator's "full" barrier
 //   warps 2-5   epilogue: tcgen05.ld of the accumulators (double-buffered), bias, GELU,
@@ -41,13 +41,13 @@ constexpr int kPlaneBytes = kBY * kRowBytes;             // one chunk of one pla
 constexpr int kChunkBytes = 3 * kPlaneBytes;             // one chunk of the block: 8640 B
 constexpr int kBoxBytes = 2 * kChunkBytes;               // bytes one TMA box delivers: 17280
 constexpr int kStageBytes = 17408;                       // stage pitch, a multiple of 128 B
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kTapBytes = 512;                           // 16 co x 16 ci, BF16
 constexpr int kWBytes = kNTaps * kTapBytes;              // 13824 B
-constexpr int kCtl = kStages * kStageBytes + kWBytes;    // control block offset (83456)
+constexpr int kCtl = kStages * kStageBytes + kWBytes;    // control block offset (66048)
 constexpr int kSmemTC = kCtl + 256 + 1024;               // + barriers + alignment slack
 constexpr int kThreadsTC = 192;
-constexpr int kCtaPerSm = 2;
+constexpr int kCtaPerSm = 3;
 constexpr int kChains = 2;                               // independent accumulators per tile (taps mod 2)
 constexpr int kAccCols = kChains * 16;                   // TMEM columns of one accumulator set
 constexpr int kTmemCols = 2 * kAccCols;                  // double-buffered: 64 columns
@@ -93,26 +93,29 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+// One try_wait with a suspend-time hint: the thread sleeps in hardware until the phase
+// completes or about `hint_ns` have passed (no busy spinning).
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
       : "memory");
   return ok != 0u;
 }
 
 // Wait for the phase of parity `parity`; false after kWaitNs or when *abort_flag is set.
+// The timer is read once per 64 sleeps of at most 1 ms each.
 __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
-  if (mbar_test(bar, parity)) return true;
+  if (mbar_test(bar, parity, 1000000u)) return true;
   const unsigned long long t0 = gtime();
-  for (;;) {
-    if (mbar_test(bar, parity)) return true;
+  for (unsigned k = 1;; ++k) {
+    if (mbar_test(bar, parity, 1000000u)) return true;
     if (abort_flag && *abort_flag) return false;
-    if (gtime() - t0 > kWaitNs) return false;
+    if ((k & 63u) == 0u && gtime() - t0 > kWaitNs) return false;
   }
 }
 
@@ -251,10 +254,11 @@ __global__ void __launch_bounds__(kThreadsTC, kCtaPerSm) k_conv_tc(const __grid_
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      // ---- MMA issuer ----
+      // ---- MMA issuer (one thread) ----
       // kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major, N = 16, M = 128
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kCh >> 3) << 17) |
-                             ((uint32_t)(kTM >> 4) << 24);
+      constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kCh >> 3) << 17) |
+                                 ((uint32_t)(kTM >> 4) << 24);
+      const uint64_t bdesc0 = sdesc(wsm, 256, 128);
       int j = 0;
       for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++j) {
         const int s = j % kStages, b = j & 1;
@@ -265,13 +269,16 @@ __global__ void __launch_bounds__(kThreadsTC, kCtaPerSm) k_conv_tc(const __grid_
           break;
         }
         tc_fence_after();
-        const uint32_t st = sbase + s * kStageBytes;
-#pragma unroll 1
+        const uint64_t adesc0 = sdesc(sbase + s * kStageBytes, kChunkBytes, kRowBytes);
+        const uint32_t d0 = tmem + b * kAccCols;
+        // fully unrolled: tap (dx, dy, dz) = (tap % 3, tap / 3 % 3, tap / 9) is a compile-time
+        // shift of the A start address (descriptor field in 16-B units); B = the tap's
+        // 512-B weight block.  The issue loop is then descriptor adds and MMAs only.
+#pragma unroll
         for (int tap = 0; tap < kNTaps; ++tap) {
-          const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-          const uint64_t ad = sdesc(st + dx * 16 + dy * kRowBytes + dz * kPlaneBytes, kChunkBytes, kRowBytes);
-          const uint64_t bd = sdesc(wsm + tap * kTapBytes, 256, 128);
-          umma_bf16(tmem + b * kAccCols + (tap % kChains) * kCh, ad, bd, idesc, tap >= kChains ? 1u : 0u);
+          const uint64_t ad = adesc0 + (uint64_t)(((tap % 3) * 16 + ((tap / 3) % 3) * kRowBytes + (tap / 9) * kPlaneBytes) >> 4);
+          const uint64_t bd = bdesc0 + (uint64_t)((tap * kTapBytes) >> 4);
+          umma_bf16(d0 + (tap % kChains) * kCh, ad, bd, idesc, tap >= kChains ? 1u : 0u);
         }
         umma_commit(cb + 32 + 8 * s);   // stage s free once these MMAs have read it
         umma_commit(cb + 64 + 8 * b);   // accumulator b ready
@@ -290,7 +297,9 @@ __global__ void __launch_bounds__(kThreadsTC, kCtaPerSm) k_conv_tc(const __grid_
     int j = 0;
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++j) {
       const int b = j & 1;
-      bool ok = mbar_wait(cb + 64 + 8 * b, (j >> 1) & 1, abort_flag);
+      // one lane per warp waits; the others join it at the vote
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(cb + 64 + 8 * b, (j >> 1) & 1, abort_flag);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) {
           atomicCAS(a.err, 0, 3);
