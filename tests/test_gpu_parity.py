@@ -65,6 +65,27 @@ def test_calc_func(name, kw):
     assert np.max(np.abs(fg - fo)) <= 1e-12 * np.max(np.abs(fo))
 
 
+def test_large_grid_one_newton_iteration():
+    """F, the assembled system and the F-norm after one Newton iteration against the
+    oracle at 3.1M cells (index arithmetic and reduction partials at a larger size)."""
+    p = make_config("hetero", shape=(256, 256, 48), precon_type=0, maxout_iter=1, maxinn_iter=5)
+    g, o = gpu_solver(p), Oracle(p)
+    g.init_state(); o.init_state()
+    h = _perturbed(p, amp=0.005)
+    fg, fo = g.calc_func(h), o.calc_func(h)
+    assert np.max(np.abs(fg - fo)) <= 1e-12 * np.max(np.abs(fo))
+    g.set_state(head_new=h); o.set_state(head_new=h)
+    dg, lg, rg = g.make_matvec()
+    do, lo, ro = o.make_matvec()
+    assert np.max(np.abs(rg - ro)) <= 1e-12 * np.max(np.abs(ro))
+    assert relmax(dg, do) < 1e-6 and relmax(lg, lo) < 1e-6
+    g.init_state(); o.init_state()
+    rg_, sg = g.calc_numsol()
+    ro_, so = o.calc_numsol()
+    assert rg_ == ro_ and sg["out_iter"] == so["out_iter"] == 1
+    assert abs(sg["l2_new"] - so["l2_new"]) <= 1e-9 * so["l2_new"]
+
+
 @pytest.mark.parametrize("name,kw", [("box", dict(shape=(10, 9, 12))), ("hetero", dict(shape=(24, 20, 16)))])
 def test_make_matvec(name, kw):
     p = make_config(name, precon_type=0, **kw)
