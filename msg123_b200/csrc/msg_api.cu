@@ -123,10 +123,10 @@ static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse) {
   return MSG_OK;
 }
 
-static int solve_linalg(msg_ctx *c, double init_norm, double *x, double *last_norm) {
+static int solve_linalg(msg_ctx *c, double init_norm, double *x, double *last_norm, bool x_zero = false) {
   if (c->timing) cudaEventRecord(c->ev[3], c->stream);
   c->bnorm = init_norm;
-  int rc = solve_bicgs(c, x);
+  int rc = solve_bicgs(c, x, x_zero);
   if (rc) return rc;
   *last_norm = c->rnorm;
   if (c->timing) {
@@ -320,7 +320,7 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     MSG_CUDA(cudaMemsetAsync(c->head_change, 0, (size_t)n * 8, c->stream));
     c->conv_flag = 0;
     c->errtol = c->prm.lin_tol > 0 ? c->prm.lin_tol : c->eta;
-    if ((rc = solve_linalg(c, c->l2_pre, c->head_change, &c->l2_jnorm))) return rc;
+    if ((rc = solve_linalg(c, c->l2_pre, c->head_change, &c->l2_jnorm, true))) return rc;   // from dh = 0
     st.inner_total += c->in_iter; st.in_iter_last = c->in_iter;
     if ((rc = axpby(c, c->head_new, c->head_pre, 1.0, c->head_change, n))) return rc;
     if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;

@@ -99,7 +99,8 @@ int build_wavefront(msg_ctx *c);
 int launch_precon_dilu(msg_ctx *c);
 int launch_solve_ilu(msg_ctx *c, const double *b, double *x);
 int launch_spmv(msg_ctx *c, const double *x, double *y);
-int solve_bicgs(msg_ctx *c, double *x);      // x in/out (device), uses c->rhs, c->bnorm, c->errtol
+// x in/out (device), uses c->rhs, c->bnorm, c->errtol; x_zero: x holds zeros on entry
+int solve_bicgs(msg_ctx *c, double *x, bool x_zero = false);
 // reductions (results land in c->hpin after a sync)
 int dot(msg_ctx *c, const double *a, const double *b, int n, double *out);   // sync + host value
 // sum narr partial arrays (nparts each, consecutive in c->part) on the device; sync; host values

@@ -186,6 +186,24 @@ __global__ void __launch_bounds__(256) k_dot2(int n, const double *a, const doub
   }
 }
 
+// Start of BiCGStab from x = 0: r = r* = p = b and the partials of <r, r*> -- the same
+// values (b - A.0 = b) and the same per-block partials as the residual SpMV, two copies
+// and k_dot2 it replaces.
+__global__ void __launch_bounds__(256) k_bicg_start0(int n, const double *b, double *r, double *rs, double *p,
+                                                     double *part) {
+  __shared__ double sh[8];
+  double s0 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = b[i];
+    r[i] = v;
+    rs[i] = v;
+    p[i] = v;
+    s0 = __dadd_rn(s0, __dmul_rn(v, v));
+  }
+  double t = block_sum<256>(s0, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 __global__ void __launch_bounds__(256) k_norm1(int n, const double *a, double *part) {
   __shared__ double sh[8];
   double s0 = 0.0;
@@ -492,24 +510,32 @@ int apply_prec(msg_ctx *c, const double *r, double *z) {
 // ---------------------------------------------------------------------------------
 // solve_bicgs (Linear_solution.f90:234-493): right-preconditioned BiCGStab, x0 = x.
 // ---------------------------------------------------------------------------------
-int solve_bicgs(msg_ctx *c, double *x) {
+int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
   const int n = c->N;
   const Geo3 g = geo3(c);
   int rc;
-  // r = b - A x
   const int nb = nblk(n);
   double red[2];
-  k_spmv<0, true><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, x, c->rhs, c->r, nullptr, nullptr);
-  MSG_CHECK_LAUNCH();
-  bool need_dilu = (c->prm.precon_type == 0) || c->prm.ref_quirks;
-  if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
-  MSG_CUDA(cudaMemcpyAsync(c->rs, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
   double sk = 0.0, sk0 = 1.0e20, sk2, alpha = 0.0, beta, omega = 1.0, ts, tt;
-  if ((rc = dot(c, c->r, c->rs, n, &sk))) return rc;
+  bool need_dilu = (c->prm.precon_type == 0) || c->prm.ref_quirks;
+  if (x_zero) {
+    // x = 0 (the Newton correction starts from zero): r = r* = p = b, sk = <b, b>
+    if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
+    k_bicg_start0<<<nb, 256, 0, c->stream>>>(n, c->rhs, c->r, c->rs, c->p, c->part);
+    MSG_CHECK_LAUNCH();
+    if ((rc = finish(c, nb, 1, &sk))) return rc;
+  } else {
+    // r = b - A x
+    k_spmv<0, true><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, x, c->rhs, c->r, nullptr, nullptr);
+    MSG_CHECK_LAUNCH();
+    if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
+    MSG_CUDA(cudaMemcpyAsync(c->rs, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = dot(c, c->r, c->rs, n, &sk))) return rc;
+  }
   c->conv_flag = 0;
   for (c->in_iter = 1; c->in_iter <= c->prm.maxinn_iter; ++c->in_iter) {
     if (c->in_iter == 1) {
-      MSG_CUDA(cudaMemcpyAsync(c->p, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+      if (!x_zero) MSG_CUDA(cudaMemcpyAsync(c->p, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
     } else {
       beta = (sk / sk0) * (alpha / omega);
       k_bicg_p<<<nb, 256, 0, c->stream>>>(n, c->p, c->r, c->v, beta, omega);
