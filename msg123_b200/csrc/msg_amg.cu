@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(128) k_r_sort(int nc, const int *rptr, int *rc
 // PASS 0 counts, PASS 1 writes.  Rows with more than kHashMax distinct columns set
 // *overflow, and the caller stops coarsening at that level.
 // ---------------------------------------------------------------------------------
-constexpr int kHash = 1024, kHashMax = 700, kSpgWarps = 3;
+constexpr int kHash = 1024, kHashMax = 700, kSpgWarps = 3, kPf = 8;
 
 template <int PASS>
 __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int *ap, const int *ac, const double *av,
@@ -340,23 +340,50 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
   const unsigned mask = (unsigned)T - 1u;
   for (int t = lane; t < T; t += 32) { K[t] = -1; V[t] = 0.0; }
   __syncwarp();
-  for (int k = start; k < a1; ++k) {
-    int j;
-    double coef;
-    if (k < a0) { j = row; coef = adiag[row]; }
-    else { j = ac[k]; coef = av[k]; }
-    int b0 = bp[j], b1 = bp[j + 1];
-    for (int q = b0 + lane; q < b1; q += 32) {
-      int cc = bc[q];
-      double p = __dmul_rn(coef, bv[q]);
-      unsigned hsh = ((unsigned)cc * 2654435761u) & mask;
-      for (int probe = 0; probe < T; ++probe) {
-        int cur = atomicCAS(&K[hsh], -1, cc);
-        if (cur == -1 || cur == cc) { V[hsh] = __dadd_rn(V[hsh], p); break; }
-        hsh = (hsh + 1) & mask;
+  auto add = [&](int cc, double p) {
+    unsigned hsh = ((unsigned)cc * 2654435761u) & mask;
+    for (int probe = 0; probe < T; ++probe) {
+      int cur = atomicCAS(&K[hsh], -1, cc);
+      if (cur == -1 || cur == cc) { V[hsh] = __dadd_rn(V[hsh], p); break; }
+      hsh = (hsh + 1) & mask;
+    }
+  };
+  // kPf entries of A at a time: their B rows (up to 32 entries, one per lane) are loaded
+  // together, so the dependent loads of A's column -> B's row bounds -> B's entries overlap
+  // across entries; they are then added in entry order exactly as one at a time.
+  for (int kb = start; kb < a1; kb += kPf) {
+    int cols[kPf], lens[kPf];
+    double vals[kPf];
+#pragma unroll
+    for (int u = 0; u < kPf; ++u) {
+      const int k = kb + u;
+      lens[u] = 0; cols[u] = -1; vals[u] = 0.0;
+      if (k < a1) {
+        int j;
+        double coef;
+        if (k < a0) { j = row; coef = adiag[row]; }
+        else { j = ac[k]; coef = av[k]; }
+        const int b0 = bp[j], len = bp[j + 1] - b0;
+        lens[u] = len;
+        if (lane < len) { cols[u] = bc[b0 + lane]; vals[u] = __dmul_rn(coef, bv[b0 + lane]); }
       }
     }
-    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kPf; ++u) {
+      const int k = kb + u;
+      if (k < a1) {
+        if (lens[u] <= 32) {
+          if (lane < lens[u]) add(cols[u], vals[u]);
+        } else {   // a B row longer than the warp: the whole row again, in chunks
+          int j;
+          double coef;
+          if (k < a0) { j = row; coef = adiag[row]; }
+          else { j = ac[k]; coef = av[k]; }
+          for (int q = bp[j] + lane; q < bp[j + 1]; q += 32) add(bc[q], __dmul_rn(coef, bv[q]));
+        }
+      }
+      __syncwarp();
+    }
   }
   // compact occupied slots
   int u = 0;
