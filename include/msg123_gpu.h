@@ -87,9 +87,12 @@ typedef struct msg_params {
   double max_step;           /* cap on delt for sim_type 1                                            */
   double end_time;           /* simulation end (s)                                                    */
   int32_t guess_mode;        /* Newton initial guess: 0 = previous head (reference), 1 = linear
-                                extrapolation, 2 = learned increment (extrapolation on failure)      */
+                                extrapolation, 2 = learned increment                                  */
   int32_t guess_select;      /* guess_mode 2: 1 = start from whichever of the learned and the
-                                extrapolated guess has the smaller ||F|| (two residual evaluations) */
+                                extrapolated guess has the smaller ||F|| (two residual evaluations);
+                                a failed solve from the learned guess is redone from the
+                                extrapolation when the guess was not vetted (0) or Newton broke
+                                down (NaN, divergence), else the step is rejected as usual          */
 } msg_params_t;
 
 /* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */

@@ -434,7 +434,11 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
     }
     rc = calc_numsol(c, &st);
     if (rc < 0) return rc;
-    if (learned_try && rc != MSG_OK) {
+    // A vetted learned guess (its residual beat the extrapolation's) that then fails to
+    // converge points at the time step, not at the guess: the step is rejected as usual.
+    // An unvetted guess, or a breakdown (NaN, divergence), is retried from the extrapolation.
+    const bool breakdown = (rc == MSG_NAN || rc == MSG_DIVERGED);
+    if (learned_try && rc != MSG_OK && (!c->prm.guess_select || breakdown)) {
       // fallback: the same time step again from the plain extrapolation
       R.newton_total += st.out_iter; R.krylov_total += st.inner_total; R.back_total += st.back_total;
       c->guess_fallbacks++;
