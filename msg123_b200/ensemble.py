@@ -70,8 +70,11 @@ class Ensemble:
         return dt, stats
 
     def autotune(self, worker_candidates=(8, 16, 32, 64), probe_steps=1):
-        """Launch shapes from a median-size member, then the worker count by timing."""
+        """Launch shapes from a median-size member, then the worker count by timing.  The
+        members advance by the probe steps (the first one assembles the systems whose
+        kernels are timed)."""
         med = self.members[int(np.argsort(self.cells)[len(self.cells) // 2])]
+        self.advance(probe_steps)
         bc, bs, _ = tune(med)
         for g in self.members:
             _lib().msg_gpu_set_tuning(g.h, bc, bs)

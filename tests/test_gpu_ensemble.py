@@ -26,7 +26,7 @@ def test_ensemble_members_match_solo_runs(tmp_path, monkeypatch):
         p = make_member(40 + k)
         with GpuSolver(p, **ENSEMBLE) as g:
             g.init_state()
-            g.advance(nsteps=1 + len((2, 6)) + 2)      # warm-up + two tuning probes + timed steps
+            g.advance(nsteps=1 + 1 + len((2, 6)) + 2)  # warm-up + autotune's probe step + two worker probes + timed
             h_solo = g.get_state()["head_new"]
         h_ens = ens.members[k].get_state()["head_new"]
         assert np.max(np.abs(h_ens - h_solo)) / np.max(np.abs(h_solo)) <= 1e-12, k
