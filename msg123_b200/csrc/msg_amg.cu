@@ -338,13 +338,17 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
   int T = 32;
   while (T < 2 * m && T < kHash) T <<= 1;
   const unsigned mask = (unsigned)T - 1u;
-  for (int t = lane; t < T; t += 32) { K[t] = -1; V[t] = 0.0; }
+  for (int t = lane; t < T; t += 32) { K[t] = -1; if (PASS == 1) V[t] = 0.0; }
   __syncwarp();
+  // PASS 0 only counts distinct columns: no values are loaded, multiplied or added
   auto add = [&](int cc, double p) {
     unsigned hsh = ((unsigned)cc * 2654435761u) & mask;
     for (int probe = 0; probe < T; ++probe) {
       int cur = atomicCAS(&K[hsh], -1, cc);
-      if (cur == -1 || cur == cc) { V[hsh] = __dadd_rn(V[hsh], p); break; }
+      if (cur == -1 || cur == cc) {
+        if (PASS == 1) V[hsh] = __dadd_rn(V[hsh], p);
+        break;
+      }
       hsh = (hsh + 1) & mask;
     }
   };
@@ -360,12 +364,15 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
       lens[u] = 0; cols[u] = -1; vals[u] = 0.0;
       if (k < a1) {
         int j;
-        double coef;
-        if (k < a0) { j = row; coef = adiag[row]; }
-        else { j = ac[k]; coef = av[k]; }
+        double coef = 0.0;
+        if (k < a0) { j = row; if (PASS == 1) coef = adiag[row]; }
+        else { j = ac[k]; if (PASS == 1) coef = av[k]; }
         const int b0 = bp[j], len = bp[j + 1] - b0;
         lens[u] = len;
-        if (lane < len) { cols[u] = bc[b0 + lane]; vals[u] = __dmul_rn(coef, bv[b0 + lane]); }
+        if (lane < len) {
+          cols[u] = bc[b0 + lane];
+          if (PASS == 1) vals[u] = __dmul_rn(coef, bv[b0 + lane]);
+        }
       }
     }
 #pragma unroll
@@ -376,10 +383,10 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
           if (lane < lens[u]) add(cols[u], vals[u]);
         } else {   // a B row longer than the warp: the whole row again, in chunks
           int j;
-          double coef;
-          if (k < a0) { j = row; coef = adiag[row]; }
-          else { j = ac[k]; coef = av[k]; }
-          for (int q = bp[j] + lane; q < bp[j + 1]; q += 32) add(bc[q], __dmul_rn(coef, bv[q]));
+          double coef = 0.0;
+          if (k < a0) { j = row; if (PASS == 1) coef = adiag[row]; }
+          else { j = ac[k]; if (PASS == 1) coef = av[k]; }
+          for (int q = bp[j] + lane; q < bp[j + 1]; q += 32) add(bc[q], PASS == 1 ? __dmul_rn(coef, bv[q]) : 0.0);
         }
       }
       __syncwarp();
@@ -458,13 +465,13 @@ __global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, cons
   }
   for (int k = adiag ? a0 - 1 : a0; k < a1; ++k) {
     int j = (k < a0) ? row : ac[k];
-    double coef = (k < a0) ? adiag[row] : av[k];
+    double coef = (PASS == 0) ? 0.0 : ((k < a0) ? adiag[row] : av[k]);
     for (int q = bp[j]; q < bp[j + 1]; ++q) {
       int cc = bc[q];
-      double p = __dmul_rn(coef, bv[q]);
+      double p = (PASS == 0) ? 0.0 : __dmul_rn(coef, bv[q]);   // PASS 0 counts columns only
       int t = 0;
       while (t < u && uc[t] != cc) ++t;
-      if (t < u) uv[t] = __dadd_rn(uv[t], p);
+      if (t < u) { if (PASS == 1) uv[t] = __dadd_rn(uv[t], p); }
       else if (u < kTU) { uc[u] = cc; uv[u] = p; ++u; }
       else {
         if (PASS == 0) { longrows[atomicAdd(nlong, 1)] = row; }
@@ -472,11 +479,13 @@ __global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, cons
       }
     }
   }
-  // insertion sort by column
-  for (int a = 1; a < u; ++a) {
-    int c0 = uc[a]; double v0 = uv[a]; int b = a - 1;
-    while (b >= 0 && uc[b] > c0) { uc[b + 1] = uc[b]; uv[b + 1] = uv[b]; --b; }
-    uc[b + 1] = c0; uv[b + 1] = v0;
+  // insertion sort by column (the count pass needs none)
+  if (PASS == 1) {
+    for (int a = 1; a < u; ++a) {
+      int c0 = uc[a]; double v0 = uv[a]; int b = a - 1;
+      while (b >= 0 && uc[b] > c0) { uc[b + 1] = uc[b]; uv[b + 1] = uv[b]; --b; }
+      uc[b + 1] = c0; uv[b + 1] = v0;
+    }
   }
   if (PASS == 0) {
     int hasd = 0;
