@@ -310,16 +310,21 @@ __global__ void __launch_bounds__(128) k_r_sort(int nc, const int *rptr, int *rc
 // *overflow, and the caller stops coarsening at that level.
 // ---------------------------------------------------------------------------------
 constexpr int kHash = 1024, kHashMax = 700, kSpgWarps = 3, kPf = 8;
+constexpr int kHashSmall = 256, kSmallMaxCols = 120;   // fill-pass table for rows of <= 120 columns
 
-template <int PASS>
+// HASH = table slots per warp.  The fill pass (PASS 1) knows each row's column count from
+// the count pass: rows of at most kSmallMaxCols columns go through the kHashSmall variant
+// (a quarter of the shared memory, twice the resident warps), the others through kHash.
+template <int PASS, int HASH = kHash>
 __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int *ap, const int *ac, const double *av,
                                                            const double *adiag, const int *bp, const int *bc,
                                                            const double *bv, int split_diag, int *ocnt,
                                                            const int *cptr, int *ccol, double *cval, double *cdiag,
                                                            int *overflow, const int *rows) {
-  __shared__ int hk[kSpgWarps][kHash];
-  __shared__ double hv[kSpgWarps][kHash];
-  __shared__ int comp[kSpgWarps][kHashMax + 32];
+  constexpr int kComp = (HASH < kHashMax ? HASH : kHashMax) + 32;
+  __shared__ int hk[kSpgWarps][HASH];
+  __shared__ double hv[kSpgWarps][PASS == 1 ? HASH : 1];
+  __shared__ int comp[kSpgWarps][kComp];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int rid = blockIdx.x * kSpgWarps + w;
   if (rid >= nrows) return;
@@ -328,15 +333,21 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
   double *V = hv[w];
   int a0 = ap[row], a1 = ap[row + 1];
   int start = adiag ? a0 - 1 : a0;
-  // products of this row -> table size (load factor <= 1/2 when it fits)
   int m = 0;
-  for (int k = start + lane; k < a1; k += 32) {
-    int j = (k < a0) ? row : ac[k];
-    m += bp[j + 1] - bp[j];
+  if (PASS == 1) {
+    // columns of this row (from the count pass; + 1 for a split-off diagonal)
+    m = cptr[row + 1] - cptr[row] + (split_diag ? 1 : 0);
+    if ((HASH == kHashSmall) != (m <= kSmallMaxCols)) return;   // the other variant's row
+  } else {
+    // products of this row -> table size (load factor <= 1/2 when it fits)
+    for (int k = start + lane; k < a1; k += 32) {
+      int j = (k < a0) ? row : ac[k];
+      m += bp[j + 1] - bp[j];
+    }
+    for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
   }
-  for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
   int T = 32;
-  while (T < 2 * m && T < kHash) T <<= 1;
+  while (T < 2 * m && T < HASH) T <<= 1;
   const unsigned mask = (unsigned)T - 1u;
   for (int t = lane; t < T; t += 32) { K[t] = -1; if (PASS == 1) V[t] = 0.0; }
   __syncwarp();
@@ -400,7 +411,7 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
     unsigned bal = __ballot_sync(0xffffffffu, occ);
     if (occ) {
       int pos = u + __popc(bal & ((1u << lane) - 1));
-      if (pos < kHashMax + 32) comp[w][pos] = t;
+      if (pos < kComp) comp[w][pos] = t;
     }
     u += __popc(bal);
   }
@@ -884,7 +895,10 @@ static int spgemm(msg_ctx *c, AmgState *A, int nrows, const int *ap, const int *
                                                    *ccol, *cval, cdiag, nullptr, nullptr);
   MSG_CHECK_LAUNCH();
   if (nlong > 0) {
-    k_spgemm<1><<<(nlong + kSpgWarps - 1) / kSpgWarps, 32 * kSpgWarps, 0, s>>>(
+    k_spgemm<1, kHashSmall><<<(nlong + kSpgWarps - 1) / kSpgWarps, 32 * kSpgWarps, 0, s>>>(
+        nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr, *ccol, *cval, cdiag, A->cnt, longrows);
+    MSG_CHECK_LAUNCH();
+    k_spgemm<1, kHash><<<(nlong + kSpgWarps - 1) / kSpgWarps, 32 * kSpgWarps, 0, s>>>(
         nlong, ap, ac, av, adiag, bp, bc, bv, split_diag, nullptr, *cptr, *ccol, *cval, cdiag, A->cnt, longrows);
     MSG_CHECK_LAUNCH();
   }
