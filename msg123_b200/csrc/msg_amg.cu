@@ -56,7 +56,7 @@ struct AmgState {
   // setup scratch
   unsigned char *sflag = nullptr;
   int *has = nullptr, *st = nullptr, *flag = nullptr, *aggid = nullptr, *agg2 = nullptr, *tmpi = nullptr;
-  unsigned long long *t1 = nullptr, *t2 = nullptr;
+  unsigned long long *t0m = nullptr, *t1 = nullptr, *t2 = nullptr;
   double *tdm = nullptr;
   // mixed precision level-1 images
   float *d1f = nullptr, *lu1f = nullptr;
@@ -134,14 +134,27 @@ __global__ void k_mis_max(int n, const int *rowptr, const int *col, const unsign
   dst[i] = m;
 }
 
-__global__ void k_mis_update(int n, int *st, const unsigned long long *t2, int *undecided) {
+// Decide the undecided nodes of this round and write the next round's tuples (t0); when
+// `undecided` is given, count the nodes still undecided (one atomic per warp).
+__global__ void k_mis_update(int n, int *st, const unsigned long long *t2, unsigned long long *t0, int lev,
+                             int *undecided) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (st[i] != 1) return;
-  unsigned long long t = t2[i];
-  if ((unsigned)(t & 0xffffffffull) == (unsigned)i) st[i] = 2;
-  else if ((t >> 62) == 2ull) st[i] = 0;
-  else atomicAdd(undecided, 1);
+  bool und = false;
+  if (i < n) {
+    int s = st[i];
+    if (s == 1) {
+      unsigned long long t = t2[i];
+      if ((unsigned)(t & 0xffffffffull) == (unsigned)i) s = 2;
+      else if ((t >> 62) == 2ull) s = 0;
+      else und = true;
+      st[i] = s;
+    }
+    t0[i] = mis_tuple(s, i, lev);
+  }
+  if (undecided) {
+    unsigned b = __ballot_sync(0xffffffffu, und);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(undecided, __popc(b));
+  }
 }
 
 __global__ void k_root_flag(int n, const int *st, int *flag) {
@@ -450,10 +463,11 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm(int nrows, const int 
 
 
 // Thread-per-row variant for short rows (at most kTU distinct columns): the products
-// are summed one by one in generation order, exactly the CPU oracle's loop.  Rows
-// that need more columns are appended to `longrows` (PASS 0) or skipped (PASS 1)
-// and go through the warp kernel above.
-constexpr int kTU = 48, kTM = 64;
+// are summed one by one in generation order, exactly the CPU oracle's loop.  The column
+// set lives in registers (fully unrolled, predicated search, insert and sorting network:
+// no dynamically indexed local memory).  Rows that need more columns are appended to
+// `longrows` (PASS 0) or skipped (PASS 1) and go through the warp kernel above.
+constexpr int kTU = 16, kTM = 64;
 template <int PASS>
 __global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, const int *ac, const double *av,
                                                   const double *adiag, const int *bp, const int *bc, const double *bv,
@@ -463,6 +477,8 @@ __global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, cons
   if (row >= nrows) return;
   int uc[kTU];
   double uv[kTU];
+#pragma unroll
+  for (int t = 0; t < kTU; ++t) { uc[t] = 0x7fffffff; uv[t] = 0.0; }
   int u = 0;
   int a0 = ap[row], a1 = ap[row + 1];
   int m = 0;
@@ -480,35 +496,50 @@ __global__ void __launch_bounds__(128) k_spgemm_t(int nrows, const int *ap, cons
     for (int q = bp[j]; q < bp[j + 1]; ++q) {
       int cc = bc[q];
       double p = (PASS == 0) ? 0.0 : __dmul_rn(coef, bv[q]);   // PASS 0 counts columns only
-      int t = 0;
-      while (t < u && uc[t] != cc) ++t;
-      if (t < u) { if (PASS == 1) uv[t] = __dadd_rn(uv[t], p); }
-      else if (u < kTU) { uc[u] = cc; uv[u] = p; ++u; }
-      else {
-        if (PASS == 0) { longrows[atomicAdd(nlong, 1)] = row; }
-        return;
+      bool found = false;
+#pragma unroll
+      for (int t = 0; t < kTU; ++t)
+        if (uc[t] == cc) { if (PASS == 1) uv[t] = __dadd_rn(uv[t], p); found = true; }
+      if (!found) {
+        if (u == kTU) {   // too many columns for the register set
+          if (PASS == 0) { longrows[atomicAdd(nlong, 1)] = row; }
+          return;
+        }
+#pragma unroll
+        for (int t = 0; t < kTU; ++t)
+          if (t == u) { uc[t] = cc; uv[t] = p; }
+        ++u;
       }
-    }
-  }
-  // insertion sort by column (the count pass needs none)
-  if (PASS == 1) {
-    for (int a = 1; a < u; ++a) {
-      int c0 = uc[a]; double v0 = uv[a]; int b = a - 1;
-      while (b >= 0 && uc[b] > c0) { uc[b + 1] = uc[b]; uv[b + 1] = uv[b]; --b; }
-      uc[b + 1] = c0; uv[b + 1] = v0;
     }
   }
   if (PASS == 0) {
     int hasd = 0;
-    if (split_diag) for (int t = 0; t < u; ++t) hasd |= (uc[t] == row);
+    if (split_diag) {
+#pragma unroll
+      for (int t = 0; t < kTU; ++t) hasd |= (uc[t] == row);
+    }
     ocnt[row] = u - hasd;
     return;
   }
+  // odd-even transposition sort by column (empty slots hold INT_MAX and stay last)
+#pragma unroll
+  for (int r = 0; r < kTU; ++r) {
+#pragma unroll
+    for (int t = r & 1; t + 1 < kTU; t += 2) {
+      if (uc[t] > uc[t + 1]) {
+        int ci = uc[t]; uc[t] = uc[t + 1]; uc[t + 1] = ci;
+        double cv = uv[t]; uv[t] = uv[t + 1]; uv[t + 1] = cv;
+      }
+    }
+  }
   int o = cptr[row];
   if (split_diag) cdiag[row] = 1.0;
-  for (int t = 0; t < u; ++t) {
-    if (split_diag && uc[t] == row) { cdiag[row] = uv[t]; continue; }
-    ccol[o] = uc[t]; cval[o] = uv[t]; ++o;
+#pragma unroll
+  for (int t = 0; t < kTU; ++t) {
+    if (t < u) {
+      if (split_diag && uc[t] == row) { cdiag[row] = uv[t]; continue; }
+      ccol[o] = uc[t]; cval[o] = uv[t]; ++o;
+    }
   }
 }
 
@@ -825,7 +856,7 @@ static int dalloc(msg_ctx *c, T **p, size_t n) {
 static int ensure_scratch(msg_ctx *c, AmgState *A, size_t n, size_t nnz) {
   if (A->cap_n >= n && A->sflag) return MSG_OK;
   cudaStream_t s = c->stream;
-  void *p[] = {A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t1, A->t2, A->tdm};
+  void *p[] = {A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t0m, A->t1, A->t2, A->tdm};
   for (void *q : p) if (q) cudaFreeAsync(q, s);
   size_t cn = std::max(n, (size_t)1024);
   int rc;
@@ -837,6 +868,7 @@ static int ensure_scratch(msg_ctx *c, AmgState *A, size_t n, size_t nnz) {
   if ((rc = dalloc(c, &A->aggid, cn))) return rc;
   if ((rc = dalloc(c, &A->agg2, cn))) return rc;
   if ((rc = dalloc(c, &A->tmpi, cn + 1))) return rc;
+  if ((rc = dalloc(c, &A->t0m, cn))) return rc;
   if ((rc = dalloc(c, &A->t1, cn))) return rc;
   if ((rc = dalloc(c, &A->t2, cn))) return rc;
   if ((rc = dalloc(c, &A->tdm, cn))) return rc;
@@ -925,17 +957,20 @@ static int coarsen(msg_ctx *c, AmgState *A, int lv, int *made) {
   MSG_CHECK_LAUNCH();
   k_mis_init<<<nb(n), kThreads, 0, s>>>(n, A->has, A->st);
   MSG_CHECK_LAUNCH();
+  // t0 = tuples of the current states; t1, t2 = the two max-propagation steps
+  unsigned long long *t0 = A->t0m;
+  k_mis_tuple<<<nb(n), kThreads, 0, s>>>(n, A->st, t0, lv);
+  MSG_CHECK_LAUNCH();
   for (int round = 0; round < 64; ++round) {
-    k_mis_tuple<<<nb(n), kThreads, 0, s>>>(n, A->st, A->t2, lv);
-    MSG_CHECK_LAUNCH();
-    k_mis_max<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->t2, A->t1);
+    k_mis_max<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, t0, A->t1);
     MSG_CHECK_LAUNCH();
     k_mis_max<<<nb(n), kThreads, 0, s>>>(n, F.rowptr, F.col, A->sflag, A->t1, A->t2);
     MSG_CHECK_LAUNCH();
-    MSG_CUDA(cudaMemsetAsync(A->cnt, 0, 4, s));
-    k_mis_update<<<nb(n), kThreads, 0, s>>>(n, A->st, A->t2, A->cnt);
+    const bool check = (round & 3) == 3 || round == 63;   // a round with nothing undecided is a no-op
+    if (check) MSG_CUDA(cudaMemsetAsync(A->cnt, 0, 4, s));
+    k_mis_update<<<nb(n), kThreads, 0, s>>>(n, A->st, A->t2, t0, lv, check ? A->cnt : nullptr);
     MSG_CHECK_LAUNCH();
-    if ((round & 3) == 3 || round == 63) {   // a round with nothing undecided is a no-op
+    if (check) {
       int und = 0;
       if ((rc = read_counter(c, A, &und))) return rc;
       if (und == 0) break;
@@ -1052,8 +1087,8 @@ void amg_free(msg_ctx *c) {
   cudaStream_t s = c->stream;
   for (size_t l = 1; l < A->lv.size(); ++l) free_level(A, A->lv[l], s);
   A->lv.clear();
-  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t1, A->t2,
-               A->tdm, A->d1f, A->lu1f};
+  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t0m, A->t1,
+               A->t2, A->tdm, A->d1f, A->lu1f};
   for (void *q : p) if (q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
   if (A->hcnt) cudaFreeHost(A->hcnt);
