@@ -742,13 +742,6 @@ __device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x
   return t;
 }
 
-__device__ __forceinline__ float csr_row_h(int i, const int *rp, const int *cl, const __nv_bfloat16 *v,
-                                           const float *d, const float *x) {
-  float t = d[i] * x[i];
-  for (int k = rp[i]; k < rp[i + 1]; ++k) t += __bfloat162float(v[k]) * x[cl[k]];
-  return t;
-}
-
 template <typename TB>
 __global__ void k_jac_first_f(int n, const TB *b, const float *d, float w, float *x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -765,18 +758,38 @@ __global__ void k_res_dia_f(Dia32 A, const double *b, const float *x, float *r) 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x)
     r[i] = (float)b[i] - dia_row_f(A, i, x);
 }
+// Coarse levels: four lanes per row (lane q takes entries q, q+4, ... of the row; quad
+// shuffle sum), so a warp keeps eight rows' loads in flight instead of 32 serial walks.
+// Launch with 4 threads per row (grid4); every lane reaches the shuffles.
+__device__ __forceinline__ float csr_off_h4(int i, int q, bool live, const int *rp, const int *cl,
+                                            const __nv_bfloat16 *v, const float *x) {
+  float t = 0.f;
+  if (live)
+    for (int k = rp[i] + q; k < rp[i + 1]; k += 4) t += __bfloat162float(v[k]) * x[cl[k]];
+  t += __shfl_xor_sync(0xffffffffu, t, 1);
+  t += __shfl_xor_sync(0xffffffffu, t, 2);
+  return t;
+}
 __global__ void k_jac_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
                             const float *b, float w, const float *x, float *y) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float r = b[i] - csr_row_h(i, rp, cl, v, d, x);
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(gt >> 2), q = (int)(gt & 3);
+  const bool live = i < n;
+  const float off = csr_off_h4(i, q, live, rp, cl, v, x);
+  if (live && q == 0) {
+    const float r = b[i] - (d[i] * x[i] + off);
     y[i] = x[i] + (w * r) / d[i];
   }
 }
 __global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
                             const float *b, const float *x, float *r) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    r[i] = b[i] - csr_row_h(i, rp, cl, v, d, x);
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(gt >> 2), q = (int)(gt & 3);
+  const bool live = i < n;
+  const float off = csr_off_h4(i, q, live, rp, cl, v, x);
+  if (live && q == 0) r[i] = b[i] - (d[i] * x[i] + off);
 }
+static int grid4(int n) { return (int)(((long long)n * 4 + kThreads - 1) / kThreads); }
 __global__ void k_restrict_f(int nc, const int *rp, const int *rc, const float *rv, const float *r, float *bc) {
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
     float s = 0.f;
@@ -1257,14 +1270,14 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
     k_jac_first_f<float><<<g, kThreads, 0, s>>>(n, b, L.diag_f, w, cur);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+      k_jac_csr_h<<<grid4(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!last) {
     AmgLevel &C = A->lv[l + 1];
-    k_res_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
+    k_res_csr_h<<<grid4(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
     MSG_CHECK_LAUNCH();
     k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
     MSG_CHECK_LAUNCH();
@@ -1274,7 +1287,7 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {
-    k_jac_csr_h<<<g, kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+    k_jac_csr_h<<<grid4(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }

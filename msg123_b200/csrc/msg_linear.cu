@@ -288,12 +288,25 @@ static int fetch_partials(msg_ctx *c, int count) {
 }
 
 // Second reduction stage: block a sums part[a*nparts .. a*nparts + nparts) in a fixed
-// order (strided per thread, then a fixed tree), so every result repeats bit for bit.
+// order, so every result repeats bit for bit: each thread keeps eight running sums over
+// the strided elements (eight loads in flight instead of one dependent chain), combines
+// them in a fixed tree, then the block reduces in a fixed tree.
 __global__ void __launch_bounds__(1024) k_finish(const double *part, int nparts, double *out) {
   __shared__ double sh[1024];
   const double *p = part + (size_t)blockIdx.x * nparts;
-  double s = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s = __dadd_rn(s, p[i]);
+  constexpr int U = 8;
+  double a[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) a[u] = 0.0;
+  for (int base = threadIdx.x; base < nparts; base += U * blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = base + u * blockDim.x;
+      if (i < nparts) a[u] = __dadd_rn(a[u], p[i]);
+    }
+  }
+  const double s = __dadd_rn(__dadd_rn(__dadd_rn(a[0], a[1]), __dadd_rn(a[2], a[3])),
+                             __dadd_rn(__dadd_rn(a[4], a[5]), __dadd_rn(a[6], a[7])));
   sh[threadIdx.x] = s;
   __syncthreads();
   for (int o = 512; o > 0; o >>= 1) {
