@@ -269,7 +269,9 @@ MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *cnn, int32_t sample, double *loss, 
 /* AdamW training over the stored samples */
 MSG_API int msg_gpu_cnn_train(msg_cnn_t *cnn, int32_t iters, float lr, float weight_decay, int32_t seed,
                               double *mean_loss);
-/* use the network in a context (guess_mode = 2); NULL detaches */
+/* use the network in a context (guess_mode = 2); NULL detaches.  One network may serve
+   several contexts, also from several host threads: their guesses take turns on it.  Do
+   not change or train its weights while attached contexts advance. */
 MSG_API int msg_gpu_cnn_attach(msg_ctx_t *ctx, msg_cnn_t *cnn);
 /* learned guesses replaced by the extrapolation after a failed Newton solve */
 MSG_API int msg_gpu_guess_fallbacks(msg_ctx_t *ctx);

@@ -20,6 +20,7 @@
 #include "msg_conv_tc.cuh"
 #include <cuda_bf16.h>
 #include <vector>
+#include <mutex>
 #include <cmath>
 #include <algorithm>
 
@@ -46,6 +47,10 @@ struct Net {
   __nv_bfloat16 *wt16 = nullptr;       // [kLayers][kWl]  mirrored taps, transposed
   __nv_bfloat16 *wtc = nullptr;        // [kLayers][kTaps][2][16][8] tensor-core operand layout
   ConvPlan *plan = nullptr;            // padded activations + TMA maps of the inference grid
+  // One network may be attached to several contexts (e.g. ensemble members driven by
+  // concurrent worker threads): the inference buffers are the network's, so each guess
+  // holds this lock until its stream has finished with them.
+  std::recursive_mutex mu;
   float *m = nullptr, *v = nullptr, *grad = nullptr;
   float *part = nullptr;               // weight-gradient partials
   int part_cap = 0;
@@ -468,6 +473,7 @@ bool learned_ready(msg_ctx *c) { return c->learned != nullptr; }
 // *s_out / *ratio_out: the increment scale and the dt ratio the features were made with.
 int learned_forward(msg_ctx *c, const float **out, double *s_out, double *ratio_out) {
   Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  std::lock_guard<std::recursive_mutex> lk(n.mu);
   int rc;
   double ss = host_sumsq_diff(c, c->head_old, c->head_old2, &rc);
   if (rc) return rc;
@@ -485,15 +491,21 @@ int learned_forward(msg_ctx *c, const float **out, double *s_out, double *ratio_
 
 int learned_convs(msg_ctx *c) {
   Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  std::lock_guard<std::recursive_mutex> lk(n.mu);
   const float *o = nullptr;
   return cnn_forward_tc(n, c->stream, &o);
 }
 
-int learned_check(msg_ctx *c) { return conv_check(reinterpret_cast<msg_cnn *>(c->learned)->net.plan, c->stream); }
+int learned_check(msg_ctx *c) {
+  Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  std::lock_guard<std::recursive_mutex> lk(n.mu);
+  return conv_check(n.plan, c->stream);
+}
 
 // head_new <- h_old + r (h_old - h_old2) + s * CNN(features)
 int learned_guess(msg_ctx *c) {
   Net &n = reinterpret_cast<msg_cnn *>(c->learned)->net;
+  std::lock_guard<std::recursive_mutex> lk(n.mu);   // held until conv_check has synchronised
   const float *o = nullptr;
   double s = 0.0, ratio = 0.0;
   int rc = learned_forward(c, &o, &s, &ratio);
@@ -661,6 +673,7 @@ MSG_API int msg_gpu_cnn_loss_grad(msg_cnn_t *h, int32_t sample, double *loss, fl
 // Inference pass of the tensor-core path on one stored sample: out = N floats.
 static int cnn_infer(msg_cnn_t *h, int32_t sample, float *out, int withhold) {
   if (!h || !out || sample < 0 || sample >= (int)h->net.data.size()) return MSG_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(h->net.mu);
   Net &n = h->net;
   Sample &smp = n.data[sample];
   int rc;
