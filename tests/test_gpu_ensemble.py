@@ -32,3 +32,33 @@ def test_ensemble_members_match_solo_runs(tmp_path, monkeypatch):
         assert np.max(np.abs(h_ens - h_solo)) / np.max(np.abs(h_solo)) <= 1e-12, k
     print("ensemble", rate, info, newton)
     ens.close()
+
+
+def test_ensemble_members_share_one_network():
+    """One CNN attached to every member, members advanced by concurrent worker threads
+    (guess_mode = 2): each member ends where it ends when advanced alone with that network."""
+    from msg123_b200.ensemble import Ensemble, ENSEMBLE
+    from msg123_b200.learned import Cnn
+    from msg123_b200.solver import GpuSolver
+    from msg123_b200.train_guess import load
+    cnn = load(Cnn(seed=0))
+    kw = dict(guess_mode=2, guess_select=0)
+    ens = Ensemble(nmembers=4, seed0=60, **kw)
+    for g in ens.members:
+        cnn.attach(g)
+    ens.init_state()
+    dt, stats = ens.advance(4, workers=4)
+    assert all(s["status"] == 0 and s["accepted"] == 4 for s in stats)
+    for k in range(4):
+        p = make_member(60 + k)
+        o = dict(ENSEMBLE)
+        o.update(kw)
+        with GpuSolver(p, **o) as g:
+            cnn.attach(g)
+            g.init_state()
+            g.advance(nsteps=4)
+            h_solo = g.get_state()["head_new"]
+        h_ens = ens.members[k].get_state()["head_new"]
+        assert np.max(np.abs(h_ens - h_solo)) / np.max(np.abs(h_solo)) <= 1e-12, k
+    ens.close()
+    cnn.close()
