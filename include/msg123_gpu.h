@@ -120,6 +120,23 @@ typedef struct msg_run_stats {
   double delt;               /* delt after the last step                  */
 } msg_run_stats_t;
 
+/* One Newton iteration, as a line of the reference's convergence log (written inside
+   calc_numsol, Nonlinear_solution.f90:59-63,240-252).  Scaled as the reference prints them. */
+typedef struct msg_convrec {
+  double time;               /* current time of the step being solved (s)                       */
+  double delt;               /* its time step (s)                                               */
+  int32_t out_iter;          /* OUTER                                                           */
+  int32_t in_iter;           /* INNER: Krylov iterations of this Newton iteration               */
+  int32_t back_iter;         /* BACK: line-search backtracks                                    */
+  int32_t cell;              /* 1-based local cell number of the largest change (maxnun)        */
+  double maxvar;             /* MAXIMUM CHANGE: signed largest head change * len_scal           */
+  double dmat;               /* DIAGONAL MATRIX at that cell * len_scal^2                       */
+  double rhs;                /* RIGHT HAND VECTOR at that cell * len_scal^3                     */
+  double head;               /* UNKNOWN VALUE: head at that cell * len_scal                     */
+  int32_t status;            /* -1: the solve went on; else the solve's status (MSG_OK, ...)    */
+  int32_t pad;
+} msg_convrec_t;
+
 typedef struct msg_ctx msg_ctx_t;
 
 /* Last error message of this thread. */
@@ -206,6 +223,12 @@ MSG_API int msg_gpu_read_restart(const char *path, int32_t ncalc, double len_sca
 /* Device time spent in the last advance/numsol call split by phase (ms):
  * [0] assembly, [1] Krylov, [2] AMG setup, [3] residual evaluations, [4] total. */
 MSG_API int msg_gpu_timers(msg_ctx_t *ctx, double *ms5);
+/* Convergence log: with on = 1 every Newton iteration of calc_numsol / advance appends one
+   msg_convrec_t to a buffer held by the context (three 8-byte device reads per iteration).
+   msg_gpu_convlog moves up to `cap` records, oldest first, into `out` and returns how many
+   (>= 0); the buffer keeps at most 2^20 records and drops the oldest beyond that. */
+MSG_API int msg_gpu_set_convlog(msg_ctx_t *ctx, int32_t on);
+MSG_API int msg_gpu_convlog(msg_ctx_t *ctx, msg_convrec_t *out, int32_t cap);
 /* Time `reps` back-to-back launches of one kernel class on the context's stream with
  * CUDA events, inputs = the current state: 0 = stencil SpMV (FP64), 1 = calc_func,
  * 2 = make_matvec, 3 = one preconditioner apply, 4 = AMG setup.  Result in ms per launch. */

@@ -78,6 +78,19 @@ class MsgRunStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MsgConvRec(C.Structure):
+    """One Newton iteration of the convergence log (msg_convrec_t)."""
+    _fields_ = [
+        ("time", C.c_double), ("delt", C.c_double),
+        ("out_iter", C.c_int32), ("in_iter", C.c_int32), ("back_iter", C.c_int32), ("cell", C.c_int32),
+        ("maxvar", C.c_double), ("dmat", C.c_double), ("rhs", C.c_double), ("head", C.c_double),
+        ("status", C.c_int32), ("pad", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 def fptr(a):
     """float32 numpy array -> POINTER(c_float) (None passes NULL)."""
     return None if a is None else a.ctypes.data_as(PF)

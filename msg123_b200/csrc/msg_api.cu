@@ -12,6 +12,7 @@
 #include <cstring>
 #include <cstdio>
 #include <vector>
+#include <deque>
 #include <atomic>
 #include <new>
 #include <string>
@@ -294,6 +295,36 @@ static int copy_d2d(msg_ctx *c, double *dst, const double *src, int n) {
   return MSG_OK;
 }
 
+constexpr size_t kConvLogMax = (size_t)1 << 20;
+using ConvLog = std::deque<msg_convrec_t>;
+
+// One line of the convergence log (Nonlinear_solution.f90:240-252): the values at the
+// cell of the largest change, scaled as the reference writes them.
+static int convlog_push(msg_ctx *c, int maxnun) {
+  msg_convrec_t r;
+  memset(&r, 0, sizeof(r));
+  r.time = c->current_t; r.delt = c->delt;
+  r.out_iter = c->out_iter; r.in_iter = c->in_iter; r.back_iter = c->back_iter;
+  r.cell = maxnun;
+  r.maxvar = c->maxvar * c->len_scal;
+  r.status = -1;
+  if (maxnun >= 1 && maxnun <= c->N) {
+    double v[3];
+    MSG_CUDA(cudaMemcpyAsync(&v[0], c->dmat + (maxnun - 1), 8, cudaMemcpyDeviceToHost, c->stream));
+    MSG_CUDA(cudaMemcpyAsync(&v[1], c->rhs + (maxnun - 1), 8, cudaMemcpyDeviceToHost, c->stream));
+    MSG_CUDA(cudaMemcpyAsync(&v[2], c->head_new + (maxnun - 1), 8, cudaMemcpyDeviceToHost, c->stream));
+    MSG_CUDA(cudaStreamSynchronize(c->stream));
+    const double L = c->len_scal;
+    r.dmat = v[0] * (L * L);
+    r.rhs = v[1] * (L * L * L);
+    r.head = v[2] * L;
+  }
+  ConvLog &q = *reinterpret_cast<ConvLog *>(c->clog);
+  if (q.size() >= kConvLogMax) q.pop_front();
+  q.push_back(r);
+  return MSG_OK;
+}
+
 // calc_numsol (Nonlinear_solution.f90:33-294)
 static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
   const int n = c->N;
@@ -350,6 +381,7 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     else if ((rc = func_norm(c, c->head_new, c->new_f, &c->l2_new))) return rc;
     st.back_total += c->back_iter; st.back_iter_last = c->back_iter;
     double conv_var = c->maxvar * c->len_scal;
+    if (c->clog_on && (rc = convlog_push(c, maxnun))) return rc;
     if (c->conv_flag == 1) {
       if ((rc = copy_d2d(c, c->surf_head, c->head_new, c->S))) return rc;   // calc_surfw
       status = MSG_OK;
@@ -363,6 +395,10 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     }
   }
   if (c->out_iter > c->prm.maxout_iter) c->out_iter = c->prm.maxout_iter;
+  if (c->clog_on && status != MSG_NAN) {   // the reference writes no line for a NaN update
+    ConvLog &q = *reinterpret_cast<ConvLog *>(c->clog);
+    if (!q.empty()) q.back().status = status;
+  }
   st.status = status; st.out_iter = c->out_iter; st.maxnun = maxnun;
   st.maxvar = c->maxvar * c->len_scal; st.l2_new = c->l2_new;
   if (stx) *stx = st;
@@ -840,6 +876,23 @@ int msg_gpu_calc_mass(msg_ctx_t *c, double *out9) {
   return MSG_OK;
 }
 
+int msg_gpu_set_convlog(msg_ctx_t *c, int32_t on) {
+  if (!c) return MSG_ERR_ARG;
+  if (on && !c->clog) c->clog = new (std::nothrow) ConvLog();
+  if (on && !c->clog) { set_error("set_convlog: out of host memory"); return MSG_ERR_SIZE; }
+  c->clog_on = on ? 1 : 0;
+  return MSG_OK;
+}
+
+int msg_gpu_convlog(msg_ctx_t *c, msg_convrec_t *out, int32_t cap) {
+  if (!c || cap < 0 || (cap > 0 && !out)) return MSG_ERR_ARG;
+  if (!c->clog) return 0;
+  ConvLog &q = *reinterpret_cast<ConvLog *>(c->clog);
+  int k = 0;
+  while (k < cap && !q.empty()) { out[k++] = q.front(); q.pop_front(); }
+  return k;
+}
+
 int msg_gpu_timers(msg_ctx_t *c, double *ms5) {
   if (!c || !ms5) return MSG_ERR_ARG;
   for (int k = 0; k < 5; ++k) ms5[k] = c->t_ms[k];
@@ -945,6 +998,8 @@ int msg_gpu_set_timing(msg_ctx_t *c, int32_t on) {
 namespace msg {
 static void free_ctx(msg_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
+  delete reinterpret_cast<ConvLog *>(c->clog);
+  c->clog = nullptr;
   amg_free(c);
   learned_free(c);
   void *dp[] = {c->reta, c->retn, c->resi, c->poro, c->ss, c->ksz, c->cell_top, c->cell_vol, c->hy, c->ab,

@@ -69,6 +69,9 @@ struct msg_ctx {
   int timestep_num, last_conv, last_out;
   int guess_fallbacks;                           // learned guesses replaced by extrapolation
   int guess_rejected;                            // learned guesses not used (larger residual)
+  // convergence log (msg_gpu_set_convlog): records of the Newton iterations, oldest first
+  void *clog;                                    // std::deque<msg_convrec_t> (msg_api.cu)
+  int clog_on;
   // learned initial guess (msg_learned.cu)
   void *learned;
   // ---- timing ------------------------------------------------------------------------------------

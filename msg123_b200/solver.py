@@ -184,6 +184,25 @@ class GpuSolver:
                                                           "surf_head"))), "get_state")
         return out
 
+    def set_convlog(self, on=True):
+        """Record every Newton iteration (the reference's convergence-log line)."""
+        L = load_library()
+        L.msg_gpu_set_convlog.argtypes = [C.c_void_p, C.c_int32]
+        _check(L.msg_gpu_set_convlog(self.h, 1 if on else 0), "set_convlog")
+
+    def convlog(self):
+        """Recorded iterations since the last call, oldest first (list of dicts); see
+        msg123_b200.convlog for writing them in the reference's format."""
+        L = load_library()
+        L.msg_gpu_convlog.argtypes = [C.c_void_p, C.POINTER(abi.MsgConvRec), C.c_int32]
+        out = []
+        buf = (abi.MsgConvRec * 4096)()
+        while True:
+            k = _check(L.msg_gpu_convlog(self.h, buf, 4096), "convlog")
+            out.extend(buf[i].as_dict() for i in range(k))
+            if k < 4096:
+                return out
+
     def guess_fallbacks(self):
         """Learned guesses whose Newton run failed and was redone from the extrapolation."""
         L = load_library()

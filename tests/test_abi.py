@@ -34,7 +34,8 @@ def test_nm_exports_match_header():
 
 
 @pytest.mark.parametrize("name,cls", [("msg_grid_t", abi.MsgGrid), ("msg_params_t", abi.MsgParams),
-                                      ("msg_stats_t", abi.MsgStats), ("msg_run_stats_t", abi.MsgRunStats)])
+                                      ("msg_stats_t", abi.MsgStats), ("msg_run_stats_t", abi.MsgRunStats),
+                                      ("msg_convrec_t", abi.MsgConvRec)])
 def test_struct_layout_matches_header(tmp_path, name, cls):
     fields = [f for f, _ in cls._fields_]
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void){',
