@@ -155,7 +155,7 @@ def make_problem(args, rank):
 # learned guess used directly (no residual check: it costs two residual evaluations per step
 # and rarely rejects a guess in this window); a failed solve from it is redone from the
 # plain extrapolation
-FAST = dict(precision=1, amg_lag=4, guess_mode=2, guess_select=0)
+FAST = dict(precision=1, amg_lag=4, guess_mode=2, guess_select=0, vg_form=1)
 PLAIN = dict(precision=0, amg_lag=0, guess_mode=0)
 
 
@@ -166,7 +166,7 @@ def workload_config(args, prob):
             "solver": "Newton (Eisenstat-Walker, cubic line search) + BiCGStab + smoothed-aggregation AMG",
             "value_path": "mixed precision (FP32 V-cycle, BF16 coarse operators, FP64 Krylov/Newton/coarse LU) + "
                           "learned initial guess (used directly, extrapolation fallback), AMG hierarchy rebuilt every 4 "
-                          "time steps",
+                          "time steps, two-pow form of Mualem kr (vg_form 1)",
             "baseline_path": "plain FP64, AMG rebuilt every Newton iteration, Newton from the previous head",
             "newton_tol": "max|dh| <= 1e-8 max|h|",
             "l2": "inputs larger than L2 (126 MB); no flush needed",

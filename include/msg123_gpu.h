@@ -93,6 +93,11 @@ typedef struct msg_params {
                                 a failed solve from the learned guess is redone from the
                                 extrapolation when the guess was not vetted (0) or Newton broke
                                 down (NaN, divergence), else the step is rejected as usual          */
+  int32_t vg_form;           /* Mualem kr: 0 = the reference's expression (four pow per cell);
+                                1 = the same function with Se^(1/m) = 1/(1+beta) and
+                                beta^m = (alpha|h|)^(n-1): two pow per cell; differs from 0 by
+                                rounding only                                                     */
+  int32_t pad;
 } msg_params_t;
 
 /* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */

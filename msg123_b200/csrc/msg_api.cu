@@ -599,6 +599,7 @@ int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t
   if ((double)grid->nx * grid->ny * grid->nz > 2.0e9 / 6.0) { set_error("grid too large for int32 CSR"); return MSG_ERR_SIZE; }
   if (params->len_scal <= 0 || params->ini_step <= 0) { set_error("len_scal and ini_step must be positive"); return MSG_ERR_ARG; }
   if (params->maxout_iter < 1 || params->maxinn_iter < 1) { set_error("iteration caps must be >= 1"); return MSG_ERR_ARG; }
+  if (params->vg_form != 0 && params->vg_form != 1) { set_error("vg_form must be 0 or 1"); return MSG_ERR_ARG; }
   const void *req[] = {grid->reta, grid->retn, grid->resi, grid->poro, grid->ss, grid->ksx, grid->ksy, grid->ksz,
                        grid->cell_top, grid->cell_vol, grid->dis2face, grid->face_area, grid->surf_top, grid->surf_bott};
   for (auto q : req) if (!q) { set_error("required grid array is NULL"); return MSG_ERR_ARG; }

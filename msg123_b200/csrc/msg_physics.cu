@@ -148,6 +148,15 @@ struct VG {
   double S, kr, alp;
 };
 
+// FORM 0 evaluates Mualem's kr = Se^(1/2) (1 - (1 - Se^(1/m))^m)^2 as the reference writes
+// it.  FORM 1 evaluates the same function with two of its four pow calls replaced by
+// identities of the van Genuchten curve: Se = (1 + beta)^-m, so Se^(1/m) = 1/(1 + beta) and
+// (1 - Se^(1/m))^m = (beta / (1 + beta))^m = Se * beta^m, with beta^m = a^(n m) = a^(n-1)
+// = beta / a (a = alpha |h|, n m = n - 1).  S is the same in both forms; kr differs by
+// rounding (relative 1e-15 where kr is near 1, growing as 1e-16 / (1 - Se beta / a) in dry
+// cells, where both forms cancel).  The limits agree: beta = 0 gives t = 1, Se = 0 gives
+// kr = 0.
+template <int FORM = 0>
 __device__ __forceinline__ VG vg_eval(double pres, double top, double pertur, float reta, float retn,
                                       float resi, float poro, float ss) {
   VG o;
@@ -155,11 +164,18 @@ __device__ __forceinline__ VG vg_eval(double pres, double top, double pertur, fl
   if (per_phead < 0.0) {
     double rn = (double)retn;
     double retm = __dsub_rn(1.0, __ddiv_rn(1.0, rn));
-    double beta = pow(fabs(__dmul_rn(per_phead, (double)reta)), rn);
+    double a = fabs(__dmul_rn(per_phead, (double)reta));
+    double beta = pow(a, rn);
     double se = pow(__dadd_rn(1.0, beta), -retm);
     double theta = __dadd_rn((double)resi, __dmul_rn((double)(poro - resi), se));
     o.S = __ddiv_rn(theta, (double)poro);
-    double t = __dsub_rn(1.0, pow(__dsub_rn(1.0, pow(se, __ddiv_rn(1.0, retm))), retm));
+    double t;
+    if (FORM == 0) {
+      t = __dsub_rn(1.0, pow(__dsub_rn(1.0, pow(se, __ddiv_rn(1.0, retm))), retm));
+    } else {
+      double ym = (beta == 0.0 || se == 0.0) ? 0.0 : __dmul_rn(se, __ddiv_rn(beta, a));
+      t = __dsub_rn(1.0, ym);
+    }
     o.kr = __dmul_rn(sqrt(se), __dmul_rn(t, t));
     o.alp = 0.0;
   } else {
@@ -170,13 +186,14 @@ __device__ __forceinline__ VG vg_eval(double pres, double top, double pertur, fl
   return o;
 }
 
+template <int FORM>
 __global__ void k_srat_rperm(int N, const double *__restrict__ h, double pertur, const double *__restrict__ top,
                              const float *__restrict__ reta, const float *__restrict__ retn,
                              const float *__restrict__ resi, const float *__restrict__ poro,
                              const float *__restrict__ ss, double *srat, double *kr, double *alp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  VG v = vg_eval(h[i], top[i], pertur, reta[i], retn[i], resi[i], poro[i], ss[i]);
+  VG v = vg_eval<FORM>(h[i], top[i], pertur, reta[i], retn[i], resi[i], poro[i], ss[i]);
   srat[i] = v.S;
   kr[i] = v.kr;
   if (alp) alp[i] = v.alp;
@@ -196,7 +213,7 @@ struct CellArgs {
 // and the storage term at h are already in srat / kr / sto from a residual evaluation at
 // the same h (the previous Newton iteration ends with one), so only the perturbed
 // evaluation at h + newper is made -- the same values bit for bit, half the pow calls.
-template <bool ASM, bool REUSE = false>
+template <bool ASM, bool REUSE = false, int FORM = 0>
 __global__ void k_cell(int N, CellArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -206,7 +223,7 @@ __global__ void k_cell(int N, CellArgs a) {
     VG v;
     v.S = a.srat[i];
     v.alp = (__dsub_rn(hi, top) < 0.0) ? 0.0 : (double)ss;   // vg_eval's branch at pertur = 0
-    VG w = vg_eval(hi, top, a.newper, reta, retn, resi, poro, ss);
+    VG w = vg_eval<FORM>(hi, top, a.newper, reta, retn, resi, poro, ss);
     a.kr_per[i] = w.kr;
     double deri_srat = __dmul_rn(__dsub_rn(w.S, v.S), a.newper_inv);
     double deri_stor = __dmul_rn(__dmul_rn(v.alp, deri_srat), hi);
@@ -214,7 +231,7 @@ __global__ void k_cell(int N, CellArgs a) {
     a.stod[i] = __dmul_rn(__dmul_rn(-x, a.delt_inv), a.vol[i]);
     return;
   }
-  VG v = vg_eval(hi, top, 0.0, reta, retn, resi, poro, ss);
+  VG v = vg_eval<FORM>(hi, top, 0.0, reta, retn, resi, poro, ss);
   double vol = a.vol[i];
   double ch1 = __dmul_rn(__dmul_rn(v.alp, a.s_old[i]), a.h_old[i]);
   double ch2 = __dmul_rn(__dmul_rn(v.alp, v.S), hi);
@@ -223,7 +240,7 @@ __global__ void k_cell(int N, CellArgs a) {
   a.srat[i] = v.S;
   a.kr[i] = v.kr;
   if (ASM) {
-    VG w = vg_eval(hi, top, a.newper, reta, retn, resi, poro, ss);
+    VG w = vg_eval<FORM>(hi, top, a.newper, reta, retn, resi, poro, ss);
     a.kr_per[i] = w.kr;
     double deri_srat = __dmul_rn(__dsub_rn(w.S, v.S), a.newper_inv);
     double deri_stor = __dmul_rn(__dmul_rn(v.alp, deri_srat), hi);
@@ -511,8 +528,9 @@ int build_connectivity(msg_ctx *c, const msg_grid_t *g) {
 }
 
 int launch_srat_rperm(msg_ctx *c, const double *h, double pertur, double *srat, double *kr, double *alp) {
-  k_srat_rperm<<<nblk(c->N), kThreads, 0, c->stream>>>(c->N, h, pertur, c->cell_top, c->reta, c->retn, c->resi,
-                                                        c->poro, c->ss, srat, kr, alp);
+  auto k = c->prm.vg_form ? k_srat_rperm<1> : k_srat_rperm<0>;
+  k<<<nblk(c->N), kThreads, 0, c->stream>>>(c->N, h, pertur, c->cell_top, c->reta, c->retn, c->resi, c->poro, c->ss,
+                                            srat, kr, alp);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -544,7 +562,8 @@ static CellArgs cell_args(msg_ctx *c, const double *h) {
 
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
   const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
-  k_cell<false><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, h));
+  auto k = c->prm.vg_form ? k_cell<false, false, 1> : k_cell<false, false, 0>;
+  k<<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, h));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, h);
   a.F = F;
@@ -556,8 +575,9 @@ int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
 
 int launch_make_matvec(msg_ctx *c, bool reuse) {
   const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
-  if (reuse) k_cell<true, true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
-  else k_cell<true><<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
+  auto k = c->prm.vg_form ? (reuse ? k_cell<true, true, 1> : k_cell<true, false, 1>)
+                           : (reuse ? k_cell<true, true, 0> : k_cell<true, false, 0>);
+  k<<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, c->head_new);
   a.F = c->rhs;

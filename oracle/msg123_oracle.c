@@ -236,7 +236,17 @@ static void srat_rperm(const orc_t *o, double pertur, const double *pres, double
       }
       srat[i] = theta / (double)o->poro[i];
       double se = pow(DONE + beta, -retm);
-      double t = DONE - pow(DONE - pow(se, DONE / retm), retm);
+      double t;
+      if (!o->prm.vg_form) {
+        t = DONE - pow(DONE - pow(se, DONE / retm), retm);
+      } else {
+        /* vg_form 1 (an option of the GPU library, not of the reference): the same kr
+         * with Se^(1/m) = 1/(1+beta) and (1 - Se^(1/m))^m = Se * beta / a, a = alpha|h|
+         * (beta^m = a^(n m) = a^(n-1)); beta = 0 gives t = 1 as above. */
+        double a = fabs(per_phead * (double)o->reta[i]);
+        double ym = (beta == DZERO || se == DZERO) ? DZERO : se * (beta / a);
+        t = DONE - ym;
+      }
       kr = sqrt(se) * (t * t);
       ss = DZERO;
     } else {

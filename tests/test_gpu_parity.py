@@ -38,9 +38,10 @@ def test_connectivity_bitexact(name, kw):
     assert np.array_equal(a["abyd"], b["abyd"])
 
 
-def test_srat_rperm():
+@pytest.mark.parametrize("vg_form", [0, 1])
+def test_srat_rperm(vg_form):
     p = make_config("hetero", shape=(20, 16, 12), seed=7)
-    g, o = gpu_solver(p), Oracle(p)
+    g, o = gpu_solver(p, vg_form=vg_form), Oracle(p, vg_form=vg_form)
     rng = np.random.default_rng(0)
     h = p.cell_top + rng.uniform(-0.2, 0.02, p.ncalc)
     for pert in (0.0, 1.19e-9):
@@ -51,14 +52,32 @@ def test_srat_rperm():
         assert np.array_equal(ssg, sso)
 
 
+def test_srat_rperm_forms_agree():
+    """vg_form 1 is the reference's kr up to rounding: S identical; kr within 1e-10
+    relative where kr > 1e-6 and 1e-16 absolute below (both forms cancel in 1 - (...) as
+    kr -> 0, so the relative difference grows as 1e-16 / t there; the oracle's two forms
+    differ by 1.3e-11 relative and 4e-19 absolute on these heads)."""
+    p = make_config("hetero", shape=(20, 16, 12), seed=7)
+    g0, g1 = gpu_solver(p, vg_form=0), gpu_solver(p, vg_form=1)
+    rng = np.random.default_rng(2)
+    h = p.cell_top - 10.0 ** rng.uniform(-6, 1.5, p.ncalc)
+    s0, k0, _ = g0.srat_rperm(h)
+    s1, k1, _ = g1.srat_rperm(h)
+    assert np.array_equal(s0, s1)
+    big = k0 > 1e-6
+    assert np.max(np.abs(k1 - k0)[big] / k0[big]) < 1e-10
+    assert np.max(np.abs(k1 - k0)[~big]) < 1e-16
+
+
 def _perturbed(p, seed=1, amp=0.01):
     return p.head0 + amp * np.random.default_rng(seed).standard_normal(p.ncalc)
 
 
+@pytest.mark.parametrize("vg_form", [0, 1])
 @pytest.mark.parametrize("name,kw", [("box", dict(shape=(10, 9, 12))), ("hetero", dict(shape=(24, 20, 16)))])
-def test_calc_func(name, kw):
+def test_calc_func(name, kw, vg_form):
     p = make_config(name, **kw)
-    g, o = gpu_solver(p), Oracle(p)
+    g, o = gpu_solver(p, vg_form=vg_form), Oracle(p, vg_form=vg_form)
     g.init_state(); o.init_state()
     h = _perturbed(p)
     fg, fo = g.calc_func(h), o.calc_func(h)
@@ -86,9 +105,10 @@ def test_large_grid_one_newton_iteration():
     assert abs(sg["l2_new"] - so["l2_new"]) <= 1e-9 * so["l2_new"]
 
 
+@pytest.mark.parametrize("vg_form", [0, 1])
 @pytest.mark.parametrize("name,kw", [("box", dict(shape=(10, 9, 12))), ("hetero", dict(shape=(24, 20, 16)))])
-def test_make_matvec(name, kw):
-    p = make_config(name, precon_type=0, **kw)
+def test_make_matvec(name, kw, vg_form):
+    p = make_config(name, precon_type=0, vg_form=vg_form, **kw)
     g, o = gpu_solver(p), Oracle(p)
     g.init_state(); o.init_state()
     h = _perturbed(p, amp=0.005)

@@ -43,6 +43,33 @@ def test_vg_closed_forms():
             assert ss[k] == 0.0
 
 
+def test_vg_form1_closed_form_and_trajectory():
+    """vg_form 1 (the library's two-pow kr) against the same closed form, and a time loop
+    with it against the reference form: the same Newton and Krylov counts, heads within
+    1e-12."""
+    p = make_config("box", shape=(2, 2, 3), vg_form=1)
+    o = Oracle(p)
+    psi = np.array([-1e-3, -0.1, -1.0, -3.0, -10.0, 0.0, 0.5, -0.02, -0.3, -5.0, 2.0, -7.0])
+    s, kr, ss = o.srat_rperm(p.cell_top + psi)
+    a, n = float(p.reta[0]), float(p.retn[0])
+    thr, ths = float(p.resi[0]), float(p.poro[0])
+    for k in range(12):
+        if psi[k] < 0:
+            se, kk = vg_closed_form(psi[k], a, n, thr, float(F32(ths - thr)) + thr)
+            assert kr[k] == pytest.approx(kk, rel=1e-10)
+    runs = []
+    for form in (0, 1):
+        q = make_config("hetero", shape=(16, 12, 10), seed=11, vg_form=form)
+        o = Oracle(q)
+        o.init_state()
+        rc, st = o.advance(nsteps=4)
+        runs.append((rc, st, o.get_state()["head_new"]))
+    (r0, s0, h0), (r1, s1, h1) = runs
+    assert r0 == r1 == 0
+    assert (s0["newton_total"], s0["krylov_total"]) == (s1["newton_total"], s1["krylov_total"])
+    assert np.max(np.abs(h1 - h0)) <= 1e-12 * np.max(np.abs(h0))
+
+
 def test_hydrostatic_equilibrium_is_exact():
     p = make_config("hetero", shape=(6, 5, 4), rain_mm_h=0.0)
     o = Oracle(p)
