@@ -48,7 +48,10 @@ def test_srat_rperm(vg_form):
         sg, kg, ssg = g.srat_rperm(h, pert)
         so, ko, sso = o.srat_rperm(h, pert)
         assert relmax(sg, so) < 1e-14
-        assert np.max(np.abs(kg - ko) / np.maximum(np.abs(ko), 1e-300)) < 1e-13
+        # CUDA's pow and the host's may differ in the last bit; form 1 carries that
+        # through Se * beta / a into 1 - (...), which cancels for the driest cells here
+        # (kr ~ 1e-6), so its bound is 1e-12 (measured 1.6e-13)
+        assert np.max(np.abs(kg - ko) / np.maximum(np.abs(ko), 1e-300)) < (1e-13 if vg_form == 0 else 1e-12)
         assert np.array_equal(ssg, sso)
 
 
