@@ -170,7 +170,8 @@ def workload_config(args, prob):
             "baseline_path": "plain FP64, AMG rebuilt every Newton iteration, Newton from the previous head",
             "newton_tol": "max|dh| <= 1e-8 max|h|",
             "l2": "inputs larger than L2 (126 MB); no flush needed",
-            "parallelism": f"replicas x{args.gpus}"}
+            "parallelism": f"replicas x{args.gpus}",
+            **({"overrides": dict(kv.split("=", 1) for kv in args.set)} if args.set else {})}
 
 
 def timed_advance(g, steps):
@@ -234,7 +235,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="override a solver parameter of the value path (e.g. amg_lag=8)")
     args = ap.parse_args()
+    from msg123_b200.config import default_params
+    for kv in args.set:
+        k, v = kv.split("=", 1)
+        FAST[k] = type(default_params()[k])(float(v) if "." in v or "e" in v else int(v))
     if args.impl == "reference":
         return run_reference(args)
 
