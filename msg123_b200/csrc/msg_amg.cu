@@ -760,25 +760,69 @@ __global__ void k_res_dia_f(Dia32 A, const double *b, const float *x, float *r) 
 }
 // Coarse levels: four lanes per row (lane q takes entries q, q+4, ... of the row; quad
 // shuffle sum), so a warp keeps eight rows' loads in flight instead of 32 serial walks.
-// Launch with 4 threads per row (grid4); every lane reaches the shuffles.
+// Each lane issues the column and value loads of four of its entries before it gathers
+// x for any of them, and the four gathers before it adds: one memory round trip per
+// four entries instead of one per entry (a row of 16 entries is one round trip).  The
+// products are still added in entry order.  Launch with 4 threads per row (grid4);
+// every lane reaches the shuffles.
 __device__ __forceinline__ float csr_off_h4(int i, int q, bool live, const int *rp, const int *cl,
                                             const __nv_bfloat16 *v, const float *x) {
   float t = 0.f;
-  if (live)
-    for (int k = rp[i] + q; k < rp[i + 1]; k += 4) t += __bfloat162float(v[k]) * x[cl[k]];
+  if (live) {
+    const int e = rp[i + 1];
+    for (int k = rp[i] + q; k < e; k += 16) {
+      int c[4];
+      float a[4], xv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int kk = k + 4 * u;
+        c[u] = kk < e ? cl[kk] : -1;
+        a[u] = kk < e ? __bfloat162float(v[kk]) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u] >= 0) t += a[u] * xv[u];
+    }
+  }
   t += __shfl_xor_sync(0xffffffffu, t, 1);
   t += __shfl_xor_sync(0xffffffffu, t, 2);
   return t;
+}
+
+// Sequential sum of one CSR row of float weights against a gathered vector, loads issued
+// four entries at a time (same order of additions as the plain loop).
+__device__ __forceinline__ float csr_row_f4(int beg, int end, const int *cl, const float *val, const float *x) {
+  float s = 0.f;
+  for (int k = beg; k < end; k += 4) {
+    int c[4];
+    float a[4], xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int kk = k + u;
+      c[u] = kk < end ? cl[kk] : -1;
+      a[u] = kk < end ? val[kk] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (c[u] >= 0) s += a[u] * xv[u];
+  }
+  return s;
 }
 __global__ void k_jac_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
                             const float *b, float w, const float *x, float *y) {
   const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(gt >> 2), q = (int)(gt & 3);
   const bool live = i < n;
+  float bi = 0.f, di = 1.f, xi = 0.f;
+  if (live && q == 0) { bi = b[i]; di = d[i]; xi = x[i]; }   // in flight during the row walk
   const float off = csr_off_h4(i, q, live, rp, cl, v, x);
   if (live && q == 0) {
-    const float r = b[i] - (d[i] * x[i] + off);
-    y[i] = x[i] + (w * r) / d[i];
+    const float r = bi - (di * xi + off);
+    y[i] = xi + (w * r) / di;
   }
 }
 __global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bfloat16 *v, const float *d,
@@ -786,22 +830,20 @@ __global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bflo
   const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(gt >> 2), q = (int)(gt & 3);
   const bool live = i < n;
+  float bi = 0.f, di = 0.f, xi = 0.f;
+  if (live && q == 0) { bi = b[i]; di = d[i]; xi = x[i]; }
   const float off = csr_off_h4(i, q, live, rp, cl, v, x);
-  if (live && q == 0) r[i] = b[i] - (d[i] * x[i] + off);
+  if (live && q == 0) r[i] = bi - (di * xi + off);
 }
 static int grid4(int n) { return (int)(((long long)n * 4 + kThreads - 1) / kThreads); }
 __global__ void k_restrict_f(int nc, const int *rp, const int *rc, const float *rv, const float *r, float *bc) {
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int q = rp[I]; q < rp[I + 1]; ++q) s += rv[q] * r[rc[q]];
-    bc[I] = s;
-  }
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x)
+    bc[I] = csr_row_f4(rp[I], rp[I + 1], rc, rv, r);
 }
 __global__ void k_prolong_f(int nf, const int *pp, const int *pc, const float *pv, const float *xc, float *x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int q = pp[i]; q < pp[i + 1]; ++q) s += pv[q] * xc[pc[q]];
-    x[i] += s;
+    const float xi = x[i];
+    x[i] = xi + csr_row_f4(pp[i], pp[i + 1], pc, pv, xc);
   }
 }
 // coarsest level: FP64 dense inverse applied to a float right-hand side
@@ -1279,7 +1321,7 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
     AmgLevel &C = A->lv[l + 1];
     k_res_csr_h<<<grid4(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
+    k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, l + 1, C.bf, C.xf);
     if (rc) return rc;
@@ -1322,7 +1364,7 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
     AmgLevel &C = A->lv[1];
     k_res_dia_f<<<gs, bs, 0, s>>>(D, b, cur, A->r0f);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<std::min(nb(C.n), kRedBlocks * 4), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
+    k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, 1, C.bf, C.xf);
     if (rc) return rc;
