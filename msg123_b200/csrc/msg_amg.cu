@@ -52,7 +52,8 @@ struct AmgState {
   size_t cap_n = 0;              // scratch capacity (rows)
   size_t sflag_cap = 0;
   double *r0 = nullptr, *t0 = nullptr;   // level-1 V-cycle work vectors
-  float *x0f = nullptr, *t0f = nullptr, *r0f = nullptr;   // level-1 FP32 work vectors (precision = 1)
+  float *x0f = nullptr, *t0f = nullptr, *r0f = nullptr;   // level-1 FP32 work vectors (precision >= 1)
+  float *b0f = nullptr;                                   // FP32 rounding of the cycle's right-hand side
   // setup scratch
   unsigned char *sflag = nullptr;
   int *has = nullptr, *st = nullptr, *flag = nullptr, *aggid = nullptr, *agg2 = nullptr, *tmpi = nullptr;
@@ -721,24 +722,32 @@ __global__ void k_gemv(int n, const double *Ci, const double *b, double *x) {
 // ---------------------------------------------------------------------------------
 // Mixed-precision V-cycle (precision = 1): FP32 vectors, FP32 level-1 operator and
 // transfer weights, BF16 off-diagonals and FP32 diagonal on the coarse levels, FP64
-// dense inverse at the coarsest level.  The Krylov recurrences stay FP64: the input r
+// dense inverse at the coarsest level.  precision = 2 also stores the level-1
+// off-diagonals in BF16 (FP32 diagonal).  The Krylov recurrences stay FP64: the input r
 // is read as double and the output z written as double.
 // ---------------------------------------------------------------------------------
-struct Dia32 {
+// Fine-level operator of the mixed V-cycle: FP32 diagonal, off-diagonals in FP32
+// (precision 1) or BF16 (precision 2), face-major like lu.
+template <typename TL>
+struct DiaT {
   int nx, ny, nz, nxy, N;
-  const float *d, *lu;
+  const float *d;
+  const TL *lu;
 };
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-__device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x) {
+template <typename TL>
+__device__ __forceinline__ float dia_row_f(const DiaT<TL> &A, int i, const float *x) {
   int iz = i / A.nxy, rem = i - iz * A.nxy, iy = rem / A.nx, ix = rem - iy * A.nx;
   const size_t N = A.N;
   float t = A.d[i] * x[i];
-  if (iz > 0) t += A.lu[0 * N + i] * x[i - A.nxy];
-  if (iy > 0) t += A.lu[1 * N + i] * x[i - A.nx];
-  if (ix > 0) t += A.lu[2 * N + i] * x[i - 1];
-  if (ix < A.nx - 1) t += A.lu[3 * N + i] * x[i + 1];
-  if (iy < A.ny - 1) t += A.lu[4 * N + i] * x[i + A.nx];
-  if (iz < A.nz - 1) t += A.lu[5 * N + i] * x[i + A.nxy];
+  if (iz > 0) t += to_f(A.lu[0 * N + i]) * x[i - A.nxy];
+  if (iy > 0) t += to_f(A.lu[1 * N + i]) * x[i - A.nx];
+  if (ix > 0) t += to_f(A.lu[2 * N + i]) * x[i - 1];
+  if (ix < A.nx - 1) t += to_f(A.lu[3 * N + i]) * x[i + 1];
+  if (iy < A.ny - 1) t += to_f(A.lu[4 * N + i]) * x[i + A.nx];
+  if (iz < A.nz - 1) t += to_f(A.lu[5 * N + i]) * x[i + A.nxy];
   return t;
 }
 
@@ -747,16 +756,30 @@ __global__ void k_jac_first_f(int n, const TB *b, const float *d, float w, float
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = (w * (float)b[i]) / d[i];
 }
-template <typename TY>
-__global__ void k_jac_dia_f(Dia32 A, const double *b, float w, const float *x, TY *y) {
+// First fine-level sweep from x = 0; also stores the FP32 rounding of the FP64 right-hand
+// side, which every later fine sweep of the cycle reads instead of rounding b again (the
+// same values, half the bytes).
+__global__ void k_jac_first_b(int n, const double *b, const float *d, float w, float *x, float *bf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float bi = (float)b[i];
+    bf[i] = bi;
+    x[i] = (w * bi) / d[i];
+  }
+}
+__global__ void k_b2f(int n, const double *b, float *bf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) bf[i] = (float)b[i];
+}
+template <typename TL, typename TY>
+__global__ void k_jac_dia_f(DiaT<TL> A, const float *b, float w, const float *x, TY *y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x) {
-    float r = (float)b[i] - dia_row_f(A, i, x);
+    float r = b[i] - dia_row_f(A, i, x);
     y[i] = (TY)(x[i] + (w * r) / A.d[i]);
   }
 }
-__global__ void k_res_dia_f(Dia32 A, const double *b, const float *x, float *r) {
+template <typename TL>
+__global__ void k_res_dia_f(DiaT<TL> A, const float *b, const float *x, float *r) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x)
-    r[i] = (float)b[i] - dia_row_f(A, i, x);
+    r[i] = b[i] - dia_row_f(A, i, x);
 }
 // Coarse levels: four lanes per row (lane q takes entries q, q+4, ... of the row; quad
 // shuffle sum), so a warp keeps eight rows' loads in flight instead of 32 serial walks.
@@ -1142,7 +1165,7 @@ void amg_free(msg_ctx *c) {
   cudaStream_t s = c->stream;
   for (size_t l = 1; l < A->lv.size(); ++l) free_level(A, A->lv[l], s);
   A->lv.clear();
-  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t0m, A->t1,
+  void *p[] = {A->col0, A->val0, A->cnt, A->r0, A->t0, A->x0f, A->t0f, A->r0f, A->b0f, A->sflag, A->has, A->st, A->flag, A->aggid, A->agg2, A->tmpi, A->t0m, A->t1,
                A->t2, A->tdm, A->d1f, A->lu1f};
   for (void *q : p) if (q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
@@ -1164,10 +1187,11 @@ int amg_setup(msg_ctx *c) {
     if ((rc = dalloc(c, &A->cnt, 1))) return rc;
     if ((rc = dalloc(c, &A->r0, c->N))) return rc;
     if ((rc = dalloc(c, &A->t0, c->N))) return rc;
-    if (c->prm.precision == 1) {
+    if (c->prm.precision >= 1) {
       if ((rc = dalloc(c, &A->x0f, c->N))) return rc;
       if ((rc = dalloc(c, &A->t0f, c->N))) return rc;
       if ((rc = dalloc(c, &A->r0f, c->N))) return rc;
+      if ((rc = dalloc(c, &A->b0f, c->N))) return rc;
     }
     MSG_CUDA(cudaMallocHost((void **)&A->hcnt, 4));
     k_col0<<<nb(c->nnz), kThreads, 0, s>>>(c->nnz, c->offrow, A->col0);
@@ -1203,7 +1227,7 @@ int amg_setup(msg_ctx *c) {
   if (A->lv.size() > 1 && A->lv.back().n <= std::max(c->prm.amg_coarse_max, 1)) {
     if ((rc = dense_inverse(c, A->lv.back()))) return rc;
   }
-  if (c->prm.precision == 1) {
+  if (c->prm.precision >= 1) {
     for (size_t l = 1; l < A->lv.size(); ++l) {
       AmgLevel &L = A->lv[l];
       int nf = A->lv[l - 1].n;
@@ -1338,31 +1362,33 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
 }
 
 // Level 1 of the mixed V-cycle: r (FP64 Krylov vector) in, z (FP64) out.
-static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
+template <typename TL>
+static int vcycle_mixed(msg_ctx *c, const double *b, double *z, const TL *lu) {
   AmgState *A = S(c);
   cudaStream_t s = c->stream;
   const int n = c->N, sw = std::max(c->prm.amg_sweeps, 0);
   const float w = c->prm.smooth_omega;
-  const int g = nb(n);
-  Dia32 D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, c->lu_f};
+  DiaT<TL> D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, lu};
   const bool single = (A->lv.size() == 1);
   const int bs = c->blk_smooth > 0 ? c->blk_smooth : kThreads;
   const int gs = (n + bs - 1) / bs;
-  float *cur = A->x0f, *oth = A->t0f;
+  float *cur = A->x0f, *oth = A->t0f, *bf = A->b0f;
   if (sw == 0) {
     MSG_CUDA(cudaMemsetAsync(cur, 0, (size_t)n * 4, s));
+    k_b2f<<<gs, bs, 0, s>>>(n, b, bf);
+    MSG_CHECK_LAUNCH();
   } else {
-    k_jac_first_f<double><<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur);
+    k_jac_first_b<<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur, bf);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, b, w, cur, oth);
+      k_jac_dia_f<TL, float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!single) {
     AmgLevel &C = A->lv[1];
-    k_res_dia_f<<<gs, bs, 0, s>>>(D, b, cur, A->r0f);
+    k_res_dia_f<TL><<<gs, bs, 0, s>>>(D, bf, cur, A->r0f);
     MSG_CHECK_LAUNCH();
     k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
@@ -1373,11 +1399,11 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   }
   for (int k = 0; k < sw; ++k) {
     if (k == sw - 1) {   // the last sweep writes the FP64 output
-      k_jac_dia_f<double><<<gs, bs, 0, s>>>(D, b, w, cur, z);
+      k_jac_dia_f<TL, double><<<gs, bs, 0, s>>>(D, bf, w, cur, z);
       MSG_CHECK_LAUNCH();
       return MSG_OK;
     }
-    k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, b, w, cur, oth);
+    k_jac_dia_f<TL, float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }
@@ -1388,7 +1414,8 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
 
 int amg_apply(msg_ctx *c, const double *r, double *z) {
   if (!S(c) || S(c)->lv.empty()) { set_error("AMG hierarchy not built"); return MSG_ERR_STATE; }
-  if (c->prm.precision == 1) return vcycle_mixed(c, r, z);
+  if (c->prm.precision >= 1)
+    return c->lu_h ? vcycle_mixed<__nv_bfloat16>(c, r, z, c->lu_h) : vcycle_mixed<float>(c, r, z, c->lu_f);
   return vcycle(c, 0, r, z);
 }
 
