@@ -72,8 +72,7 @@ typedef struct msg_params {
   int32_t maxinn_iter;       /* BiCGStab iteration cap                                                */
   int32_t precon_type;       /* 0: DILU / ILU(0); 1: AMG                                              */
   int32_t ref_quirks;        /* 1: AMG preconditioner reproduces the reference (output = fine DILU)    */
-  int32_t precision;         /* 0: FP64 everywhere; 1: FP32 V-cycle, BF16 coarse operators;
-                                2: as 1 with BF16 off-diagonals on the fine level too                 */
+  int32_t precision;         /* 0: FP64 everywhere; 1: FP32 V-cycle, BF16 coarse operators            */
   int32_t amg_nlevel;        /* maximum number of AMG levels                                          */
   int32_t amg_coarse_max;    /* coarsest level is solved directly once it has <= this many rows       */
   int32_t amg_sweeps;        /* Jacobi sweeps before and after the coarse correction                  */

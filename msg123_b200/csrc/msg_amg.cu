@@ -52,7 +52,7 @@ struct AmgState {
   size_t cap_n = 0;              // scratch capacity (rows)
   size_t sflag_cap = 0;
   double *r0 = nullptr, *t0 = nullptr;   // level-1 V-cycle work vectors
-  float *x0f = nullptr, *t0f = nullptr, *r0f = nullptr;   // level-1 FP32 work vectors (precision >= 1)
+  float *x0f = nullptr, *t0f = nullptr, *r0f = nullptr;   // level-1 FP32 work vectors (precision = 1)
   float *b0f = nullptr;                                   // FP32 rounding of the cycle's right-hand side
   // setup scratch
   unsigned char *sflag = nullptr;
@@ -722,32 +722,24 @@ __global__ void k_gemv(int n, const double *Ci, const double *b, double *x) {
 // ---------------------------------------------------------------------------------
 // Mixed-precision V-cycle (precision = 1): FP32 vectors, FP32 level-1 operator and
 // transfer weights, BF16 off-diagonals and FP32 diagonal on the coarse levels, FP64
-// dense inverse at the coarsest level.  precision = 2 also stores the level-1
-// off-diagonals in BF16 (FP32 diagonal).  The Krylov recurrences stay FP64: the input r
+// dense inverse at the coarsest level.  The Krylov recurrences stay FP64: the input r
 // is read as double and the output z written as double.
 // ---------------------------------------------------------------------------------
-// Fine-level operator of the mixed V-cycle: FP32 diagonal, off-diagonals in FP32
-// (precision 1) or BF16 (precision 2), face-major like lu.
-template <typename TL>
-struct DiaT {
+struct Dia32 {
   int nx, ny, nz, nxy, N;
-  const float *d;
-  const TL *lu;
+  const float *d, *lu;
 };
-__device__ __forceinline__ float to_f(float v) { return v; }
-__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-template <typename TL>
-__device__ __forceinline__ float dia_row_f(const DiaT<TL> &A, int i, const float *x) {
+__device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x) {
   int iz = i / A.nxy, rem = i - iz * A.nxy, iy = rem / A.nx, ix = rem - iy * A.nx;
   const size_t N = A.N;
   float t = A.d[i] * x[i];
-  if (iz > 0) t += to_f(A.lu[0 * N + i]) * x[i - A.nxy];
-  if (iy > 0) t += to_f(A.lu[1 * N + i]) * x[i - A.nx];
-  if (ix > 0) t += to_f(A.lu[2 * N + i]) * x[i - 1];
-  if (ix < A.nx - 1) t += to_f(A.lu[3 * N + i]) * x[i + 1];
-  if (iy < A.ny - 1) t += to_f(A.lu[4 * N + i]) * x[i + A.nx];
-  if (iz < A.nz - 1) t += to_f(A.lu[5 * N + i]) * x[i + A.nxy];
+  if (iz > 0) t += A.lu[0 * N + i] * x[i - A.nxy];
+  if (iy > 0) t += A.lu[1 * N + i] * x[i - A.nx];
+  if (ix > 0) t += A.lu[2 * N + i] * x[i - 1];
+  if (ix < A.nx - 1) t += A.lu[3 * N + i] * x[i + 1];
+  if (iy < A.ny - 1) t += A.lu[4 * N + i] * x[i + A.nx];
+  if (iz < A.nz - 1) t += A.lu[5 * N + i] * x[i + A.nxy];
   return t;
 }
 
@@ -769,15 +761,14 @@ __global__ void k_jac_first_b(int n, const double *b, const float *d, float w, f
 __global__ void k_b2f(int n, const double *b, float *bf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) bf[i] = (float)b[i];
 }
-template <typename TL, typename TY>
-__global__ void k_jac_dia_f(DiaT<TL> A, const float *b, float w, const float *x, TY *y) {
+template <typename TY>
+__global__ void k_jac_dia_f(Dia32 A, const float *b, float w, const float *x, TY *y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x) {
     float r = b[i] - dia_row_f(A, i, x);
     y[i] = (TY)(x[i] + (w * r) / A.d[i]);
   }
 }
-template <typename TL>
-__global__ void k_res_dia_f(DiaT<TL> A, const float *b, const float *x, float *r) {
+__global__ void k_res_dia_f(Dia32 A, const float *b, const float *x, float *r) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x)
     r[i] = b[i] - dia_row_f(A, i, x);
 }
@@ -1187,7 +1178,7 @@ int amg_setup(msg_ctx *c) {
     if ((rc = dalloc(c, &A->cnt, 1))) return rc;
     if ((rc = dalloc(c, &A->r0, c->N))) return rc;
     if ((rc = dalloc(c, &A->t0, c->N))) return rc;
-    if (c->prm.precision >= 1) {
+    if (c->prm.precision == 1) {
       if ((rc = dalloc(c, &A->x0f, c->N))) return rc;
       if ((rc = dalloc(c, &A->t0f, c->N))) return rc;
       if ((rc = dalloc(c, &A->r0f, c->N))) return rc;
@@ -1227,7 +1218,7 @@ int amg_setup(msg_ctx *c) {
   if (A->lv.size() > 1 && A->lv.back().n <= std::max(c->prm.amg_coarse_max, 1)) {
     if ((rc = dense_inverse(c, A->lv.back()))) return rc;
   }
-  if (c->prm.precision >= 1) {
+  if (c->prm.precision == 1) {
     for (size_t l = 1; l < A->lv.size(); ++l) {
       AmgLevel &L = A->lv[l];
       int nf = A->lv[l - 1].n;
@@ -1362,13 +1353,12 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
 }
 
 // Level 1 of the mixed V-cycle: r (FP64 Krylov vector) in, z (FP64) out.
-template <typename TL>
-static int vcycle_mixed(msg_ctx *c, const double *b, double *z, const TL *lu) {
+static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   AmgState *A = S(c);
   cudaStream_t s = c->stream;
   const int n = c->N, sw = std::max(c->prm.amg_sweeps, 0);
   const float w = c->prm.smooth_omega;
-  DiaT<TL> D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, lu};
+  Dia32 D{c->nx, c->ny, c->nz, c->nxy, c->N, c->dmat_f, c->lu_f};
   const bool single = (A->lv.size() == 1);
   const int bs = c->blk_smooth > 0 ? c->blk_smooth : kThreads;
   const int gs = (n + bs - 1) / bs;
@@ -1381,14 +1371,14 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z, const TL *lu) {
     k_jac_first_b<<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur, bf);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_dia_f<TL, float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
+      k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!single) {
     AmgLevel &C = A->lv[1];
-    k_res_dia_f<TL><<<gs, bs, 0, s>>>(D, bf, cur, A->r0f);
+    k_res_dia_f<<<gs, bs, 0, s>>>(D, bf, cur, A->r0f);
     MSG_CHECK_LAUNCH();
     k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
@@ -1399,11 +1389,11 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z, const TL *lu) {
   }
   for (int k = 0; k < sw; ++k) {
     if (k == sw - 1) {   // the last sweep writes the FP64 output
-      k_jac_dia_f<TL, double><<<gs, bs, 0, s>>>(D, bf, w, cur, z);
+      k_jac_dia_f<double><<<gs, bs, 0, s>>>(D, bf, w, cur, z);
       MSG_CHECK_LAUNCH();
       return MSG_OK;
     }
-    k_jac_dia_f<TL, float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
+    k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }
@@ -1414,8 +1404,7 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z, const TL *lu) {
 
 int amg_apply(msg_ctx *c, const double *r, double *z) {
   if (!S(c) || S(c)->lv.empty()) { set_error("AMG hierarchy not built"); return MSG_ERR_STATE; }
-  if (c->prm.precision >= 1)
-    return c->lu_h ? vcycle_mixed<__nv_bfloat16>(c, r, z, c->lu_h) : vcycle_mixed<float>(c, r, z, c->lu_f);
+  if (c->prm.precision == 1) return vcycle_mixed(c, r, z);
   return vcycle(c, 0, r, z);
 }
 

@@ -55,10 +55,6 @@ __global__ void k_vecjac_out(int n, double *out, const double *f2, const double 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[i] = __dmul_rn(-(NEG ? __dadd_rn(f2[i], f1[i]) : __dsub_rn(f2[i], f1[i])), eps_inv);
 }
-__global__ void k_to_bf16(size_t n, const double *a, __nv_bfloat16 *b) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    b[i] = __double2bfloat16(a[i]);
-}
 __global__ void k_to_f32(size_t n, const double *a, float *b) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
@@ -580,10 +576,9 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
                    &c->slope_rhs, &c->dilu_d, &c->r, &c->rs, &c->p, &c->v, &c->t, &c->z};
   for (auto q : vn) { ALLOC(*q, N * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, N * 8, c->stream)); }
   ALLOC(c->lu, 6 * N * 8);
-  if (p->precision >= 1) {
+  if (p->precision == 1) {
     ALLOC(c->dmat_f, N * 4);
-    if (p->precision == 1) ALLOC(c->lu_f, 6 * N * 4);
-    else ALLOC(c->lu_h, 6 * N * 2);
+    ALLOC(c->lu_f, 6 * N * 4);
   }
   size_t npart = std::max((size_t)kRedBlocks * 8, 2 * (size_t)nblk((int)N) + 64);
   ALLOC(c->part, npart * 8);
@@ -605,7 +600,7 @@ int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t
   if (params->len_scal <= 0 || params->ini_step <= 0) { set_error("len_scal and ini_step must be positive"); return MSG_ERR_ARG; }
   if (params->maxout_iter < 1 || params->maxinn_iter < 1) { set_error("iteration caps must be >= 1"); return MSG_ERR_ARG; }
   if (params->vg_form != 0 && params->vg_form != 1) { set_error("vg_form must be 0 or 1"); return MSG_ERR_ARG; }
-  if (params->precision < 0 || params->precision > 2) { set_error("precision must be 0, 1 or 2"); return MSG_ERR_ARG; }
+  if (params->precision != 0 && params->precision != 1) { set_error("precision must be 0 or 1"); return MSG_ERR_ARG; }
   const void *req[] = {grid->reta, grid->retn, grid->resi, grid->poro, grid->ss, grid->ksx, grid->ksy, grid->ksz,
                        grid->cell_top, grid->cell_vol, grid->dis2face, grid->face_area, grid->surf_top, grid->surf_bott};
   for (auto q : req) if (!q) { set_error("required grid array is NULL"); return MSG_ERR_ARG; }
@@ -746,8 +741,7 @@ int msg_gpu_set_system(msg_ctx_t *c, const double *dmat, const double *lumat, co
   if (c->dmat_f) {
     k_to_f32<<<kRedBlocks, kThreads, 0, c->stream>>>(N, c->dmat, c->dmat_f);
     MSG_CHECK_LAUNCH();
-    if (c->lu_f) k_to_f32<<<kRedBlocks, kThreads, 0, c->stream>>>(6 * N, c->lu, c->lu_f);
-    else k_to_bf16<<<kRedBlocks, kThreads, 0, c->stream>>>(6 * N, c->lu, c->lu_h);
+    k_to_f32<<<kRedBlocks, kThreads, 0, c->stream>>>(6 * N, c->lu, c->lu_f);
     MSG_CHECK_LAUNCH();
   }
   MSG_CUDA(cudaStreamSynchronize(c->stream));
@@ -1016,7 +1010,7 @@ static void free_ctx(msg_ctx *c) {
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,
                 c->head_change, c->srat_new, c->srat_old, c->surf_head, c->surf_old, c->new_f, c->kr, c->kr_per,
                 c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->head_old2, c->slope_rhs, c->dilu_d, c->r, c->rs,
-                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f, c->lu_h, c->dres};
+                c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f, c->dres};
   for (auto q : dp) if (q) cudaFree(q);
   if (c->hpin) cudaFreeHost(c->hpin);
   for (int k = 0; k < 8; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);

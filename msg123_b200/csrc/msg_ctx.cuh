@@ -2,7 +2,6 @@
 // between the translation units of libmsg123gpu.so.
 #pragma once
 #include "msg_common.cuh"
-#include <cuda_bf16.h>
 #include "../../include/msg123_gpu.h"
 
 namespace msg {
@@ -47,8 +46,7 @@ struct msg_ctx {
   double *tmpv;                                  // [N] spare vector (J.v, line search)
   // ---- level-1 system, DIA: lu[d*N + i] = J(i, nb_d(i)) --------------------------------
   double *dmat, *lu, *rhs, *slope_rhs;
-  float *dmat_f, *lu_f;                          // FP32 images (precision >= 1; lu_f for precision 1)
-  __nv_bfloat16 *lu_h;                           // BF16 off-diagonals of the fine level (precision 2)
+  float *dmat_f, *lu_f;                          // FP32 images (precision = 1)
   // ---- Krylov work ----------------------------------------------------------------------
   double *dilu_d, *r, *rs, *p, *v, *t, *z;
   msg::DevScalars *sc;                           // device scalars

@@ -264,7 +264,6 @@ struct FluxArgs {
   double *F;          // residual (calc_func) or rhs = -F (make_matvec)
   double *dmat, *lu;  // assembly outputs
   float *dmat_f, *lu_f;   // FP32 images for the mixed-precision V-cycle (nullable)
-  __nv_bfloat16 *lu_h;    // BF16 image of the off-diagonals (precision 2; nullable)
   double *part;       // partial sums of F^2 (nullable)
 };
 
@@ -345,7 +344,6 @@ __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
       if (ASM) {
         a.lu[(size_t)d * N + i] = luv;
         if (a.lu_f) a.lu_f[(size_t)d * N + i] = (float)luv;
-        if (a.lu_h) a.lu_h[(size_t)d * N + i] = __double2bfloat16(luv);
       }
     }
     // boundary terms of the top layer
@@ -549,7 +547,7 @@ static FluxArgs flux_args(msg_ctx *c, const double *h) {
   a.drain = c->drain;
   a.newper = c->newper; a.newper_inv = c->newper_inv;
   a.F = nullptr; a.dmat = nullptr; a.lu = nullptr; a.part = nullptr;
-  a.dmat_f = nullptr; a.lu_f = nullptr; a.lu_h = nullptr;
+  a.dmat_f = nullptr; a.lu_f = nullptr;
   return a;
 }
 
@@ -587,7 +585,6 @@ int launch_make_matvec(msg_ctx *c, bool reuse) {
   a.lu = c->lu;
   a.dmat_f = c->dmat_f;
   a.lu_f = c->lu_f;
-  a.lu_h = c->lu_h;
   a.part = c->part;
   k_flux_asm<<<nblk(c->N), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
