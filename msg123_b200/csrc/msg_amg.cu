@@ -779,8 +779,11 @@ __global__ void k_res_dia_f(Dia32 A, const float *b, const float *x, float *r) {
 // four entries instead of one per entry (a row of 16 entries is one round trip).  The
 // products are still added in entry order.  Launch with 4 threads per row (grid4);
 // every lane reaches the shuffles.
-__device__ __forceinline__ float csr_off_h4(int i, int q, bool live, const int *rp, const int *cl,
-                                            const __nv_bfloat16 *v, const float *x) {
+__device__ __forceinline__ float ldf(const float *p) { return *p; }
+__device__ __forceinline__ float ldf(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+template <typename TV>
+__device__ __forceinline__ float csr_off_h4(int i, int q, bool live, const int *rp, const int *cl, const TV *v,
+                                            const float *x) {
   float t = 0.f;
   if (live) {
     const int e = rp[i + 1];
@@ -791,7 +794,7 @@ __device__ __forceinline__ float csr_off_h4(int i, int q, bool live, const int *
       for (int u = 0; u < 4; ++u) {
         const int kk = k + 4 * u;
         c[u] = kk < e ? cl[kk] : -1;
-        a[u] = kk < e ? __bfloat162float(v[kk]) : 0.f;
+        a[u] = kk < e ? ldf(v + kk) : 0.f;
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
@@ -850,9 +853,15 @@ __global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bflo
   if (live && q == 0) r[i] = bi - (di * xi + off);
 }
 static int grid4(int n) { return (int)(((long long)n * 4 + kThreads - 1) / kThreads); }
+// Restriction b_c = R r: a coarse row gathers from every fine row its aggregate's
+// smoothed prolongation reaches (tens of entries), so it is split over four lanes like the
+// coarse-level smoother.  Launch with grid4(nc).
 __global__ void k_restrict_f(int nc, const int *rp, const int *rc, const float *rv, const float *r, float *bc) {
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x)
-    bc[I] = csr_row_f4(rp[I], rp[I + 1], rc, rv, r);
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int I = (int)(gt >> 2), q = (int)(gt & 3);
+  const bool live = I < nc;
+  const float t = csr_off_h4(I, q, live, rp, rc, rv, r);
+  if (live && q == 0) bc[I] = t;
 }
 __global__ void k_prolong_f(int nf, const int *pp, const int *pc, const float *pv, const float *xc, float *x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
@@ -860,13 +869,17 @@ __global__ void k_prolong_f(int nf, const int *pp, const int *pc, const float *p
     x[i] = xi + csr_row_f4(pp[i], pp[i + 1], pc, pv, xc);
   }
 }
-// coarsest level: FP64 dense inverse applied to a float right-hand side
+// coarsest level: FP64 dense inverse applied to a float right-hand side, one warp per
+// row (coalesced row reads, fixed shuffle tree).  Launch with n warps; a warp's row index
+// is the same in all its lanes, so a warp past the end leaves as a whole.
 __global__ void k_gemv_mixed(int n, const double *Ci, const float *b, float *x) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int row = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
   double s = 0.0;
-  for (int j = 0; j < n; ++j) s += Ci[(size_t)i * n + j] * (double)b[j];
-  x[i] = (float)s;
+  for (int j = lane; j < n; j += 32) s += Ci[(size_t)row * n + j] * (double)b[j];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) x[row] = (float)s;
 }
 __global__ void k_d2f(int n, const double *a, float *b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
@@ -1315,7 +1328,7 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
   const int g = nb(n);
   const bool last = (l == (int)A->lv.size() - 1);
   if (last && L.cinv) {
-    k_gemv_mixed<<<nb(n), kThreads, 0, s>>>(n, L.cinv, b, x);
+    k_gemv_mixed<<<(int)(((long long)n * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(n, L.cinv, b, x);
     MSG_CHECK_LAUNCH();
     return MSG_OK;
   }
@@ -1336,7 +1349,7 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
     AmgLevel &C = A->lv[l + 1];
     k_res_csr_h<<<grid4(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
+    k_restrict_f<<<grid4(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, l + 1, C.bf, C.xf);
     if (rc) return rc;
@@ -1380,7 +1393,7 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
     AmgLevel &C = A->lv[1];
     k_res_dia_f<<<gs, bs, 0, s>>>(D, bf, cur, A->r0f);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<nb(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
+    k_restrict_f<<<grid4(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, 1, C.bf, C.xf);
     if (rc) return rc;
