@@ -217,6 +217,12 @@ MSG_API int msg_gpu_advance(msg_ctx_t *ctx, int32_t nsteps, double rech_until, d
  * storage, flow, recharge, well, surface, river, lake, sea (+ out[8] drainage),
  * each a volume over the step (rate * delt). */
 MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
+/* Water table of the current state (calc_wtable, Calc_output.f90:20-52, called by
+ * write_out_wtabf with head_new and srat_new): for each surface column, the head of the
+ * lowest cell that is not fully saturated (srat != 1), scanning up from the bottom layer;
+ * the top cell's head when the whole column is saturated.  wtable: [ncals] host doubles,
+ * nondimensional like head (the reference writes wtable * len_scal). */
+MSG_API int msg_gpu_water_table(msg_ctx_t *ctx, double *wtable);
 /* Restart file in the reference's format (replaces write_rest, Nonlinear_solution.f90:792-816,
    and write_out_restf, Write_output.f90:415-432): gfortran sequential unformatted records
    [real(DP) time][head_new * len_scal, ncalc values], 4-byte length markers. */

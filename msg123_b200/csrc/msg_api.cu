@@ -878,6 +878,15 @@ int msg_gpu_calc_mass(msg_ctx_t *c, double *out9) {
   return MSG_OK;
 }
 
+int msg_gpu_water_table(msg_ctx_t *c, double *wtable) {
+  if (!c || !wtable) return MSG_ERR_ARG;
+  int rc = launch_water_table(c, c->tmpv);   // tmpv: N >= S doubles of scratch
+  if (rc) return rc;
+  MSG_CUDA(cudaMemcpyAsync(wtable, c->tmpv, (size_t)c->S * 8, cudaMemcpyDeviceToHost, c->stream));
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
 int msg_gpu_set_convlog(msg_ctx_t *c, int32_t on) {
   if (!c) return MSG_ERR_ARG;
   if (on && !c->clog) c->clog = new (std::nothrow) ConvLog();

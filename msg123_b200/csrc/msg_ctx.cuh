@@ -88,6 +88,7 @@ namespace msg {
 // ---- msg_physics.cu ---------------------------------------------------------------------------
 int build_connectivity(msg_ctx *c, const msg_grid_t *g);
 int launch_srat_rperm(msg_ctx *c, const double *h, double pertur, double *srat, double *kr, double *alp);
+int launch_water_table(msg_ctx *c, double *wt);
 // F = calc_func(h); also writes srat_new and kr (rel_perm).  partial sums of F^2 in c->part[0..].
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm);
 // make_matvec at c->head_new: dmat, lu (DIA), rhs = -F.  reuse: srat_new, kr and sto

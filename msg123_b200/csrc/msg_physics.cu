@@ -527,6 +527,28 @@ int build_connectivity(msg_ctx *c, const msg_grid_t *g) {
   return MSG_OK;
 }
 
+// calc_wtable (Calc_output.f90:20-52), one thread per surface column: walk up from the
+// bottom layer, keep the head of each cell, stop at the first cell that is not fully
+// saturated.  Layer k of column i is cell k * S + i (S = nx * ny cells per layer).
+__global__ void k_water_table(int S, int nz, const double *__restrict__ h, const double *__restrict__ srat,
+                              double *wt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  double w = 0.0;
+  for (int k = nz - 1; k >= 0; --k) {
+    const size_t cell = (size_t)k * S + i;
+    w = h[cell];
+    if (srat[cell] != 1.0) break;
+  }
+  wt[i] = w;
+}
+
+int launch_water_table(msg_ctx *c, double *wt) {
+  k_water_table<<<nblk(c->S), kThreads, 0, c->stream>>>(c->S, c->nz, c->head_new, c->srat_new, wt);
+  MSG_CHECK_LAUNCH();
+  return MSG_OK;
+}
+
 int launch_srat_rperm(msg_ctx *c, const double *h, double pertur, double *srat, double *kr, double *alp) {
   auto k = c->prm.vg_form ? k_srat_rperm<1> : k_srat_rperm<0>;
   k<<<nblk(c->N), kThreads, 0, c->stream>>>(c->N, h, pertur, c->cell_top, c->reta, c->retn, c->resi, c->poro, c->ss,

@@ -184,6 +184,15 @@ class GpuSolver:
                                                           "surf_head"))), "get_state")
         return out
 
+    def water_table(self):
+        """calc_wtable of the current state (Calc_output.f90:20-52): [ncals] heads,
+        nondimensional like head_new."""
+        L = load_library()
+        L.msg_gpu_water_table.argtypes = [C.c_void_p, abi.PD]
+        out = np.zeros(self.ncals)
+        _check(L.msg_gpu_water_table(self.h, dptr(out)), "water_table")
+        return out
+
     def set_convlog(self, on=True):
         """Record every Newton iteration (the reference's convergence-log line)."""
         L = load_library()

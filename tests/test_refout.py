@@ -1,0 +1,91 @@
+"""Output series in the reference's binary format and the water table behind one of them.
+
+CPU: the record layout of write_header_bin + write_3dbin / write_2dbin (Write_module.f90:
+61-99,146-225) -- float32 time, then float32(value * unit) x fastest -- written and read
+back; the water-table restatement (calc_wtable, Calc_output.f90:20-52) on hand-made
+columns.  GPU: the device water table equals the restatement on a solved state, and the
+three series written from that state read back as the reference would have written them.
+"""
+import numpy as np
+import pytest
+
+from msg123_b200 import refout
+from oracle.output_ref import water_table
+
+
+def test_record_layout_and_round_trip(tmp_path):
+    nx, ny, nz = 3, 2, 4
+    rng = np.random.default_rng(0)
+    h1, h2 = rng.standard_normal(nx * ny * nz), rng.standard_normal(nx * ny * nz)
+    unit = np.float32(10.0)
+    p = tmp_path / "head.bin"
+    refout.append(p, 1800.0, h1, unit, (nx, ny, nz))
+    refout.append(p, 3600.0, h2, unit, (nx, ny, nz))
+    raw = np.fromfile(p, dtype="<f4")
+    assert raw.size == 2 * (1 + nx * ny * nz)
+    assert raw[0] == np.float32(1800.0)
+    # cell (x=2, y=1, z=1) is the second value; (x=1, y=2, z=1) the fourth; (1, 1, 2) the seventh
+    assert raw[1 + 1] == np.float32(h1[1] * 10.0)
+    assert raw[1 + 3] == np.float32(h1[3] * 10.0)
+    assert raw[1 + 6] == np.float32(h1[6] * 10.0)
+    recs = refout.read(p, (nx, ny, nz))
+    assert [t for t, _ in recs] == [1800.0, 3600.0]
+    assert recs[1][1].shape == (nz, ny, nx)
+    assert np.array_equal(recs[1][1].reshape(-1), (h2 * np.float64(unit)).astype(np.float32))
+    w = tmp_path / "wtab.bin"
+    refout.append(w, 5.0, h1[: nx * ny], 1.0, (nx, ny))
+    (t, a), = refout.read(w, (nx, ny))
+    assert t == 5.0 and a.shape == (ny, nx) and np.array_equal(a.reshape(-1), h1[: nx * ny].astype(np.float32))
+    with pytest.raises(ValueError):
+        refout.read(p, (nx, ny, nz + 1))
+    with pytest.raises(ValueError):
+        refout.append(p, 0.0, h1[:-1], 1.0, (nx, ny, nz))
+
+
+def test_product_rounds_once():
+    """real(value * unit, SP): the product in double, one rounding to single."""
+    v = np.array([0.1234567890123, -3.333333333333])
+    unit = 100.0
+    assert np.array_equal(refout.field(v, unit, (2, 1)), (v * 100.0).astype(np.float32))
+
+
+def test_water_table_restatement_by_hand():
+    nx, ny, nz = 3, 1, 4
+    # columns: 0 fully saturated, 1 unsaturated at the bottom, 2 saturated below layer 1
+    srat = np.array([[1.0, 0.9, 0.8],
+                     [1.0, 0.9, 0.7],
+                     [1.0, 0.95, 1.0],
+                     [1.0, 0.99, 1.0]])
+    head = np.arange(12, dtype=np.float64).reshape(nz, nx * ny) + 0.5
+    wt = water_table(head.reshape(-1), srat.reshape(-1), nx, ny, nz)
+    assert wt[0] == head[0, 0]      # whole column saturated: top cell
+    assert wt[1] == head[3, 1]      # bottom cell already unsaturated
+    assert wt[2] == head[1, 2]      # lowest unsaturated cell above the saturated ones
+
+
+@pytest.mark.gpu
+def test_gpu_water_table_and_series(tmp_path):
+    from msg123_b200.config import make_config
+    from msg123_b200.solver import GpuSolver
+    p = make_config("hetero", shape=(24, 20, 16), seed=9)
+    g = GpuSolver(p, precision=1, amg_lag=4)
+    g.init_state()
+    rc, st = g.advance(nsteps=4)
+    assert rc == 0
+    s = g.get_state()
+    wt = g.water_table()
+    ref = water_table(s["head_new"], s["srat_new"], p.nx, p.ny, p.nz)
+    assert np.array_equal(wt, ref)
+    # the hydrostatic start puts the water table inside the block: some columns must pass
+    # saturated cells on the way up
+    assert np.any(s["srat_new"] == 1.0) and np.any(s["srat_new"] < 1.0)
+    ls = p.params["len_scal"]
+    prefix = str(tmp_path / "run")
+    refout.write_state(prefix, g, st["current_t"], ls)
+    (t, h), = refout.read(prefix + "_head.bin", (p.nx, p.ny, p.nz))
+    assert t == np.float32(st["current_t"])
+    assert np.array_equal(h.reshape(-1), (s["head_new"] * np.float64(np.float32(ls))).astype(np.float32))
+    (_, sr), = refout.read(prefix + "_srat.bin", (p.nx, p.ny, p.nz))
+    assert np.array_equal(sr.reshape(-1), s["srat_new"].astype(np.float32))
+    (_, w), = refout.read(prefix + "_wtab.bin", (p.nx, p.ny))
+    assert np.array_equal(w.reshape(-1), (ref * np.float64(np.float32(ls))).astype(np.float32))
