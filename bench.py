@@ -54,6 +54,48 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 ALG_BYTES = {0: 72.0, 1: 164.0, 2: 280.0}
 KERNEL_NAMES = {0: "stencil SpMV (FP64, DIA)", 1: "calc_func (vG pass + flux pass)",
                 2: "make_matvec (vG pair + Jacobian assembly)"}
+
+
+def vcycle_bytes(sizes, sweeps, coarse_max):
+    """Algorithmic bytes of one mixed-precision V-cycle (FP32 vectors, FP32 fine-level DIA
+    operator, BF16 coarse off-diagonals with int32 columns, FP32 transfer weights, FP64
+    dense coarsest inverse), from the level sizes [(rows, off-diagonal entries, prolongation
+    entries from the level above)], level 0 = fine grid.  Every array a kernel touches is
+    counted once per kernel; gathered vectors are counted once.
+      fine sweep        : b 4 + x 4 + d 4 + six off-diagonals 24 + out 4 = 40 B per cell
+                          (first sweep: b 8 in, d 4, x 4 and b 4 out; last: FP64 out, +4)
+      residual          : like a sweep
+      coarse sweep/res. : rowptr 4 + diagonal 4 + b 4 + x 4 + out 4 per row, col 4 + value 2
+                          per entry (first sweep: b, d, out = 12 per row)
+      restriction       : rowptr 4 per coarse row, col 4 + weight 4 per entry, fine r 4 per
+                          fine row, out 4 per coarse row; prolongation the same from the
+                          fine side plus the read-modify-write of x (8 per fine row)
+      coarsest inverse  : 8 n^2 + 8 n"""
+    sw = max(int(sweeps), 0)
+    total = 0.0
+    nl = len(sizes)
+    for lv, (n, nnz, _) in enumerate(sizes):
+        last = lv == nl - 1
+        if lv > 0 and last and n <= coarse_max:
+            total += 8.0 * n * n + 8.0 * n
+            break
+        if lv == 0:
+            sweep, res = 40.0 * n, 40.0 * n
+            first = 20.0 * n if sw else 16.0 * n
+            final = 4.0 * n if sw else 12.0 * n          # FP64 output of the last sweep / copy
+        else:
+            sweep = res = 20.0 * n + 6.0 * nnz
+            first = 12.0 * n if sw else 4.0 * n
+            final = 0.0
+        total += first + max(sw - 1, 0) * sweep + sw * sweep + final
+        if not last:
+            nc, _, pnnz = sizes[lv + 1]
+            total += res
+            total += 4.0 * nc + 8.0 * pnnz + 4.0 * n + 4.0 * nc     # restriction
+            total += 4.0 * n + 8.0 * pnnz + 4.0 * nc + 8.0 * n      # prolongation
+    return total
+
+
 # Learned-guess CNN on the tensor cores: 4 convolutions x 27 taps x 16 x 16 (channels padded
 # to 16, as the tcgen05 MMA computes them) x 2 flops per cell.
 CNN_FLOP_PER_CELL = 4 * 27 * 16 * 16 * 2
@@ -273,9 +315,13 @@ def main():
     peaks, src = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     tc_peak = float(peaks.get("bf16_tflops", 1590.0))
+    # the V-cycle first: make_matvec below re-assembles at the converged head, whose
+    # right-hand side is far smaller than any the solve passes to the preconditioner
+    t_prec = g.kernel_time(3, reps=5)
+    vc_bytes = vcycle_bytes(g.amg_sizes(), g.params["amg_sweeps"], g.params["amg_coarse_max"])
+    vc_gbs = vc_bytes / (t_prec * 1e-3) / 1e9
     kt = {w: g.kernel_time(w, reps=10) for w in (0, 1, 2)}
     gbs = {w: ALG_BYTES[w] * prob.ncalc / (kt[w] * 1e-3) / 1e9 for w in kt}
-    t_prec = g.kernel_time(3, reps=5)
     t_setup = g.kernel_time(4, reps=2)
     t_cnn = g.kernel_time(5, reps=5)
     cnn_tflops = CNN_FLOP_PER_CELL * prob.ncalc / (t_cnn * 1e-3) / 1e12
@@ -351,7 +397,10 @@ def main():
                                          for w in (0, 2)},
                                         **{"learned-guess CNN, 4 tcgen05 convolutions": {
                                             "ms": t_cnn, "TFLOP/s": cnn_tflops, "frac": cnn_tflops / tc_peak,
-                                            "bound": "tensor", "peak_TFLOP/s": tc_peak}}),
+                                            "bound": "tensor", "peak_TFLOP/s": tc_peak},
+                                           "mixed V-cycle, all levels": {
+                                            "ms": t_prec, "GB/s": vc_gbs, "frac": vc_gbs / hbm,
+                                            "alg_bytes": vc_bytes}}),
                          "vcycle_mixed_ms": t_prec, "amg_setup_ms": t_setup},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }

@@ -293,6 +293,17 @@ class GpuSolver:
         _check(load_library().msg_gpu_calc_mass(self.h, dptr(out)), "calc_mass")
         return out
 
+    def amg_sizes(self):
+        """(rows, off-diagonal entries, prolongation entries from the level above) of each
+        level of the last AMG setup, level 0 = Jacobian (its prolongation count is 0)."""
+        L = load_library()
+        out = []
+        for lv in range(L.msg_gpu_amg_nlevel(self.h)):
+            n, nnz, pnnz = C.c_int32(), C.c_int32(), C.c_int32()
+            _check(L.msg_gpu_amg_level_sizes(self.h, lv, C.byref(n), C.byref(nnz), C.byref(pnnz)), "amg sizes")
+            out.append((n.value, nnz.value, pnnz.value if lv > 0 else 0))
+        return out
+
     def amg_levels(self):
         """The AMG hierarchy of the last setup (level 0 = Jacobian), as numpy arrays."""
         L = load_library()
