@@ -242,7 +242,9 @@ MSG_API int msg_gpu_set_convlog(msg_ctx_t *ctx, int32_t on);
 MSG_API int msg_gpu_convlog(msg_ctx_t *ctx, msg_convrec_t *out, int32_t cap);
 /* Time `reps` back-to-back launches of one kernel class on the context's stream with
  * CUDA events, inputs = the current state: 0 = stencil SpMV (FP64), 1 = calc_func,
- * 2 = make_matvec, 3 = one preconditioner apply, 4 = AMG setup.  Result in ms per launch. */
+ * 2 = make_matvec, 3 = one preconditioner apply, 4 = AMG setup, 5 = the four tensor-core
+ * convolutions of the learned guess (needs an attached network and one accepted step).
+ * Result in ms per launch. */
 MSG_API int msg_gpu_kernel_time(msg_ctx_t *ctx, int32_t which, int32_t reps, double *ms_per_launch);
 
 /* AMG hierarchy of the last setup (structural tests): level 0 is the Jacobian in CSR
