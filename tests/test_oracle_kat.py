@@ -4,6 +4,7 @@ what pins the restatement):
 
 * van Genuchten / Mualem closed forms at chosen pressure heads (Calc_parameter.f90:15-77);
 * hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101);
+* a unit-gradient saturated column between a ponded top and free drainage is steady;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F;
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern;
@@ -76,6 +77,35 @@ def test_hydrostatic_equilibrium_is_exact():
     o.init_state()
     f = o.calc_func(p.head0)
     assert np.all(f == 0.0)
+
+
+def test_unit_gradient_column_is_steady():
+    """A saturated box under 1 m of ponding (sea top) with free drainage at the bottom: total
+    head falling by exactly the centre-to-centre distance per layer (the sea-face distance at
+    the top) is a steady state -- the same flux K_s A enters through the sea face, crosses
+    every layer and leaves as free drainage, and nothing moves sideways -- so F vanishes to
+    rounding (Calc_function.f90:212-254 flow, :475-513 sea term, plus the free-drainage
+    extension) and the time loop keeps it."""
+    import dataclasses
+    p = make_config("box", shape=(4, 3, 10))
+    ls = p.params["len_scal"]
+    sea = float(p.sea_head[0]) + 0.95 / ls
+    p = dataclasses.replace(p, sea_head=np.full_like(p.sea_head, sea))
+    N, nxy = p.ncalc, p.nx * p.ny
+    dis = p.dis2face.reshape(6, N)          # face-major: up, north, west, east, south, down
+    h = np.empty(N)
+    h[:nxy] = sea - dis[0, :nxy]
+    for c in range(nxy, N):
+        h[c] = h[c - nxy] - (dis[5, c - nxy] + dis[0, c])
+    assert np.min(h - p.cell_top) > 0.0     # saturated everywhere (kr = 1)
+    o = Oracle(p)
+    o.init_state(head=h)
+    o.set_state(head_new=h, head_old=h, delt=1800.0)
+    flux = float(p.ksz[0]) * float(p.face_area.reshape(6, N)[0, 0])
+    assert np.max(np.abs(o.calc_func(h))) <= 1e-14 * flux
+    rc, st = o.advance(nsteps=2)
+    assert rc == 0 and st["accepted"] == 2
+    assert np.max(np.abs(o.get_state()["head_new"] - h)) <= 1e-12 * np.max(np.abs(h))
 
 
 def test_fd_jacobian_matches_directional_derivative():
