@@ -4,7 +4,8 @@ what pins the restatement):
 
 * van Genuchten / Mualem closed forms at chosen pressure heads (Calc_parameter.f90:15-77);
 * hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101);
-* a unit-gradient saturated column between a ponded top and free drainage is steady;
+* a unit-gradient saturated column between a ponded top and free drainage is steady, and
+  an unsaturated column under recharge balances its fluxes term by term;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F;
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern;
@@ -106,6 +107,40 @@ def test_unit_gradient_column_is_steady():
     rc, st = o.advance(nsteps=2)
     assert rc == 0 and st["accepted"] == 2
     assert np.max(np.abs(o.get_state()["head_new"] - h)) <= 1e-12 * np.max(np.abs(h))
+
+
+def test_recharge_column_flux_balance():
+    """An unsaturated column (suction 0.7 m at the top) under recharge, with free drainage
+    and no sea layer: total head falls by the centre-to-centre distance per layer, so every
+    vertical flux is K_s kr_up A (upwind kr from the upper cell, calc_hyd_upwind,
+    Calc_parameter.f90:107-125) and F is the recharge (Calc_function.f90:256-275) minus the
+    outflow plus the inflow from above, with the free drainage K_s kr A at the bottom."""
+    import dataclasses
+    p = make_config("box", shape=(3, 2, 4))
+    ls = p.params["len_scal"]
+    N, nxy = p.ncalc, p.nx * p.ny
+    dis, far = p.dis2face.reshape(6, N), p.face_area.reshape(6, N)
+    h = np.empty(N)
+    h[:nxy] = p.cell_top[:nxy] - 0.7 / ls
+    for c in range(nxy, N):
+        h[c] = h[c - nxy] - (dis[5, c - nxy] + dis[0, c])
+    _, kr, _ = Oracle(dataclasses.replace(p, sea_top=0)).srat_rperm(h)
+    assert np.all(kr < 0.01)                 # well inside the unsaturated range
+    ks = float(p.ksz[0])
+    rech = ks * kr[:nxy] * far[0, :nxy]      # matches the top layer's drainage
+    q = dataclasses.replace(p, sea_top=0, rech=rech)
+    o = Oracle(q)
+    o.init_state(head=h)
+    o.set_state(head_new=h, head_old=h, delt=1800.0)
+    f = o.calc_func(h)
+    pred = np.zeros(N)
+    pred[:nxy] += rech
+    for c in range(N):
+        out = ks * kr[c] * far[5, c]
+        pred[c] -= out
+        if c + nxy < N:
+            pred[c + nxy] += out
+    assert np.max(np.abs(f - pred)) <= 1e-15 * ks * far[0, 0]
 
 
 def test_fd_jacobian_matches_directional_derivative():
