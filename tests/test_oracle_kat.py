@@ -10,7 +10,8 @@ what pins the restatement):
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern;
 * mass balance closes after a time step (Calc_function.f90:103-174);
-* connectivity layout on a 2x2x3 box written out by hand (Set_condition.f90:1584-2026).
+* connectivity layout on a 2x2x3 box written out by hand (Set_condition.f90:1584-2026), and
+  every face conductance equal to the distance-weighted harmonic mean of the two cells' K_s.
 """
 import numpy as np
 import pytest
@@ -225,3 +226,24 @@ def test_connectivity_by_hand():
     from oracle.oracle import lib
     import ctypes
     assert lib().orc_nseal(ctypes.c_void_p(o.h)) == 4
+
+
+def test_face_conductance_is_harmonic_mean():
+    """set_dis_adj + set_sat_hyd (Set_condition.f90:2111-2158): the face conductance between
+    cells i and j is the distance-weighted harmonic mean of their K_s, and area_dis is the
+    face area over the centre-to-centre distance."""
+    p = make_config("hetero", shape=(5, 4, 3), seed=21)
+    o = Oracle(p)
+    c = o.connect()
+    N = p.ncalc
+    dis, far = p.dis2face.reshape(6, N), p.face_area.reshape(6, N)
+    ks = {1: p.ksz, 2: p.ksy, 3: p.ksx, 4: p.ksx, 5: p.ksy, 6: p.ksz}
+    opp = {1: 6, 2: 5, 3: 4, 4: 3, 5: 2, 6: 1}
+    for i in range(N):
+        for k in range(c["offind"][i], c["offind"][i + 1]):
+            j, d = c["offrow"][k] - 1, int(c["conn_dir"][k])
+            d1, d2 = dis[d - 1, i], dis[opp[d] - 1, j]
+            k1, k2 = float(ks[d][i]), float(ks[d][j])
+            harm = k1 * k2 * (d1 + d2) / (d1 * k2 + d2 * k1)
+            assert c["hydf"][k] == pytest.approx(harm, rel=1e-14)
+            assert c["abyd"][k] == pytest.approx(far[d - 1, i] / (d1 + d2), rel=1e-15)
