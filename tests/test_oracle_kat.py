@@ -10,6 +10,7 @@ what pins the restatement):
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern;
 * mass balance closes after a time step (Calc_function.f90:103-174);
+* the adaptive time step follows apply_heuri's three factors (Time_module.f90:1522-1543);
 * connectivity layout on a 2x2x3 box written out by hand (Set_condition.f90:1584-2026), and
   every face conductance equal to the distance-weighted harmonic mean of the two cells' K_s.
 """
@@ -247,3 +248,25 @@ def test_face_conductance_is_harmonic_mean():
             harm = k1 * k2 * (d1 + d2) / (d1 * k2 + d2 * k1)
             assert c["hydf"][k] == pytest.approx(harm, rel=1e-14)
             assert c["abyd"][k] == pytest.approx(far[d - 1, i] / (d1 + d2), rel=1e-15)
+
+
+def test_time_step_heuristic():
+    """apply_heuri (Time_module.f90:1522-1543): after an accepted step with n Newton
+    iterations the next dt is 1.2, 1 or 0.8 times the last one for n <= int(0.4 maxout),
+    n <= int(0.8 maxout) or more, capped at max_step; the simulated time is real(SP)."""
+    p = make_config("hetero", shape=(12, 10, 8), seed=3)
+    prm = p.params
+    o = Oracle(p)
+    o.init_state()
+    incr, decr = int(prm["maxout_iter"] * 0.4), int(prm["maxout_iter"] * 0.8)
+    rc, st = o.advance(nsteps=1)
+    seen = set()
+    for _ in range(7):
+        n, dt, t = st["newton_total"], st["delt"], st["current_t"]
+        rc, st = o.advance(nsteps=1)
+        assert rc == 0 and st["rejected"] == 0
+        factor = 1.2 if n <= incr else (1.0 if n <= decr else 0.8)
+        seen.add(factor)
+        assert st["delt"] == min(dt * factor, prm["max_step"])
+        assert st["current_t"] == float(np.float32(t + st["delt"]))
+    assert len(seen) >= 2                     # the sequence exercises more than one branch
