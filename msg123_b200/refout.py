@@ -1,4 +1,5 @@
-"""Output files in the reference's binary format, written from the library's state.
+"""Files in the reference's binary formats: output series written from the library's state,
+and the plain real(SP) fields its input decks use.
 
 The reference writes its head, saturation and water-table files as unformatted stream
 files (open_new_wbin, Utility_module.f90:156-184): for each output time one record of
@@ -14,6 +15,12 @@ write_out_headf (Write_output.f90:321-366, unit len_scal), write_out_sratf (:368
 
 `append` adds one record, `read` returns the records of a file written here or by the
 Fortran build, and `write_state` writes the three series for a solver's current state.
+
+Input fields of type 6 (3D) and 4 (2D) are the same stream layout without the time
+header: read_3d_r4bin / read_2d_r4bin (Read_module.f90:266-299,446-479) read
+real(SP) field(nx, ny[, nz]) x fastest, and set_3dr4_calc (Set_condition.f90) hands value
+(x, y, z) to the cell of that grid position -- on a full grid, the local cell order.
+`write_field` / `read_field` write and read them.
 """
 import numpy as np
 
@@ -46,6 +53,24 @@ def read(path, shape):
         raise ValueError(f"read: {path} is not a series of {shape} records")
     recs = raw.reshape(-1, n + 1)
     return [(float(r[0]), r[1:].reshape(tuple(reversed(shape)))) for r in recs]
+
+
+def write_field(path, values, shape):
+    """An input field of type 6 (shape (nx, ny, nz)) or 4 (shape (nx, ny)): the values as
+    real(SP), local cell order = x fastest, no header."""
+    v = np.asarray(values, dtype=np.float32).reshape(-1)
+    if v.size != int(np.prod(shape)):
+        raise ValueError(f"write_field: {v.size} values for a {shape} grid")
+    v.astype("<f4").tofile(path)
+
+
+def read_field(path, shape):
+    """An input field written by `write_field` (or for the Fortran build), as a float32
+    array of `shape` reversed ([nz, ny, nx] or [ny, nx])."""
+    raw = np.fromfile(path, dtype="<f4")
+    if raw.size != int(np.prod(shape)):
+        raise ValueError(f"read_field: {path} holds {raw.size} values, not a {shape} grid")
+    return raw.reshape(tuple(reversed(shape)))
 
 
 def write_state(prefix, solver, time, len_scal):

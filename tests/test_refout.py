@@ -89,3 +89,15 @@ def test_gpu_water_table_and_series(tmp_path):
     assert np.array_equal(sr.reshape(-1), s["srat_new"].astype(np.float32))
     (_, w), = refout.read(prefix + "_wtab.bin", (p.nx, p.ny))
     assert np.array_equal(w.reshape(-1), (ref * np.float64(np.float32(ls))).astype(np.float32))
+
+
+def test_input_field_round_trip(tmp_path):
+    nx, ny, nz = 4, 3, 2
+    v = np.random.default_rng(1).standard_normal(nx * ny * nz).astype(np.float32)
+    p = tmp_path / "ks.bin"
+    refout.write_field(p, v, (nx, ny, nz))
+    assert p.stat().st_size == 4 * nx * ny * nz
+    a = refout.read_field(p, (nx, ny, nz))
+    assert a.shape == (nz, ny, nx) and a[1, 0, 2] == v[nx * ny + 2]
+    with pytest.raises(ValueError):
+        refout.read_field(p, (nx, ny))
