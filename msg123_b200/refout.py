@@ -18,7 +18,7 @@ Fortran build, and `write_state` writes the three series for a solver's current 
 
 Input fields of type 6 (3D) and 4 (2D) are the same stream layout without the time
 header: read_3d_r4bin / read_2d_r4bin (Read_module.f90:266-299,446-479) read
-real(SP) field(nx, ny[, nz]) x fastest, and set_3dr4_calc (Set_condition.f90) hands value
+real(SP) field(nx, ny[, nz]) x fastest, and set_3dr4_calc (Set_condition.f90:1092-1160) hands value
 (x, y, z) to the cell of that grid position -- on a full grid, the local cell order.
 `write_field` / `read_field` write and read them.
 """
