@@ -4,7 +4,6 @@ CPU: the Fortran edit descriptors (ESw.d, Iw, Aw), the header and iteration line
 the cell label of get_cnum, and a write -> read round trip.  GPU: the library records one
 entry per Newton iteration, ending with the solve's status, and the last entry agrees
 with the solve's statistics and the state."""
-import numpy as np
 import pytest
 
 from msg123_b200 import convlog

@@ -5,7 +5,6 @@ what is tested."""
 import os
 import socket
 
-import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
