@@ -6,6 +6,8 @@ bin-pack on cells x expected Newton iterations per step (the expected count grow
 the member's lnKs spread) -- builds only its own members on its GPU and advances them with
 the batched driver (msg_gpu_ensemble_advance).  Per-member statistics are gathered on the
 host at the end; throughput = all members' cells x accepted steps / the slowest rank's time.
+A rank whose members fail still joins that gather, carrying the error, so every rank stops
+with the same message instead of waiting in the collective for a rank that left.
 
 The reference runs one realisation per (MPI) job; this replaces launching many jobs.
 """
@@ -71,14 +73,21 @@ def run(nmembers, nsteps, rank=0, world_size=1, dist=None, runner=gpu_runner, se
     parts, load = assign(member_work(seeds), world_size)
     mine = [seeds[k] for k in parts[rank]]
     t0 = time.perf_counter()
-    stats, dt = runner(mine, nsteps) if mine else ([], 0.0)
+    err = None
+    try:
+        stats, dt = runner(mine, nsteps) if mine else ([], 0.0)
+    except Exception as e:   # reported to every rank by the gather below, which all ranks reach
+        stats, dt, err = [], 0.0, f"{type(e).__name__}: {e}"
     wall = time.perf_counter() - t0
-    local = {"rank": rank, "members": parts[rank], "stats": stats, "seconds": dt, "wall": wall}
+    local = {"rank": rank, "members": parts[rank], "stats": stats, "seconds": dt, "wall": wall, "error": err}
     if dist is not None and world_size > 1:
         gathered = [None] * world_size
         dist.all_gather_object(gathered, local)
     else:
         gathered = [local]
+    failed = [(g["rank"], g["error"]) for g in gathered if g["error"]]
+    if failed:
+        raise RuntimeError("ensemble failed on " + "; ".join(f"rank {r}: {m}" for r, m in failed))
     per_member = [None] * nmembers
     for g in gathered:
         for k, s in zip(g["members"], g["stats"]):

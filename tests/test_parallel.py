@@ -73,3 +73,43 @@ def test_gloo_two_ranks_shard_and_gather():
     expected = sum(s["cells"] * 3 for s in o0["stats"]) / max(0.01 * len(p) for p in o0["parts"])
     assert o0["throughput"] == pytest.approx(expected)
     assert res[0][1] == res[1][1] == 2.5 and res[0][2] == res[1][2] == 4.0
+
+
+def _failing_runner(seeds, nsteps):
+    import torch.distributed as dist
+    if dist.get_rank() == 1:
+        raise ValueError("member build failed")
+    return fake_runner(seeds, nsteps)
+
+
+def _failing_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        parallel.run(8, 2, rank=rank, world_size=world, dist=dist, runner=_failing_runner)
+        q.put((rank, None))
+    except RuntimeError as e:
+        q.put((rank, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_rank_failure_reaches_every_rank():
+    """Rank 1 raises while building its members: both ranks end with the same error, well
+    inside the process group's timeout (no rank waits in the gather for the failed one)."""
+    import time
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    t0 = time.time()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert time.time() - t0 < 50
+    assert res[0] == res[1] and "rank 1: ValueError: member build failed" in res[0]
