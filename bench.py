@@ -166,7 +166,9 @@ def dist_setup():
     rank = int(os.environ["RANK"])
     local = int(os.environ.get("LOCAL_RANK", rank))
     torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    # short enough that ranks left waiting for a failed one end with an error soon; the
+    # longest gap between two collectives (field generation, context build) is seconds
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     return rank, ws, dist
 
 
