@@ -314,10 +314,13 @@ static int convlog_push(msg_ctx *c, int maxnun) {
     MSG_CUDA(cudaMemcpyAsync(&v[1], c->rhs + (maxnun - 1), 8, cudaMemcpyDeviceToHost, c->stream));
     MSG_CUDA(cudaMemcpyAsync(&v[2], c->head_new + (maxnun - 1), 8, cudaMemcpyDeviceToHost, c->stream));
     MSG_CUDA(cudaStreamSynchronize(c->stream));
-    const double L = c->len_scal;
-    r.dmat = v[0] * (L * L);
-    r.rhs = v[1] * (L * L * L);
-    r.head = v[2] * L;
+    // len_scal is real(SP) in the reference, so len_scal**2 and **3 are single-precision
+    // products (Nonlinear_solution.f90:245-247) before they scale the double values
+    const float Lf = (float)c->len_scal;
+    const float L2 = Lf * Lf, L3 = L2 * Lf;
+    r.dmat = v[0] * (double)L2;
+    r.rhs = v[1] * (double)L3;
+    r.head = v[2] * c->len_scal;
   }
   ConvLog &q = *reinterpret_cast<ConvLog *>(c->clog);
   if (q.size() >= kConvLogMax) q.pop_front();
