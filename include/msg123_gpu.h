@@ -228,7 +228,8 @@ MSG_API int msg_gpu_water_table(msg_ctx_t *ctx, double *wtable);
    [real(DP) time][head_new * len_scal, ncalc values], 4-byte length markers. */
 MSG_API int msg_gpu_write_restart(msg_ctx_t *ctx, const char *path);
 /* Reads such a file (replaces the restart branch of assign_initv, Assign_calculation.f90:416-434):
-   head = value * (1 / len_scal); host code only, no GPU needed. */
+   head = value * len_scal_inv with len_scal_inv = 1/len_scal rounded to single precision (as
+   Read_input.f90:1108 forms it), time rounded to single precision; host code only, no GPU. */
 MSG_API int msg_gpu_read_restart(const char *path, int32_t ncalc, double len_scal, double *head, double *time);
 
 /* Device time spent in the last advance/numsol call split by phase (ms):

@@ -864,9 +864,11 @@ int msg_gpu_read_restart(const char *path, int32_t ncalc, double len_scal, doubl
   const bool ok = get_record(f, &t, 8) && get_record(f, head, (size_t)ncalc * 8);
   fclose(f);
   if (!ok) { set_error("read_restart: %s is not a restart file of %d cells", path, ncalc); return MSG_ERR_SIZE; }
-  const double inv = 1.0 / len_scal;
+  // assign_initv multiplies by len_scal_inv = SONE/len_scal, a real(SP) reciprocal
+  // (Read_input.f90:1108, Assign_calculation.f90:433), and keeps the time as real(SP) (:431)
+  const double inv = (double)(1.0f / (float)len_scal);
   for (int32_t i = 0; i < ncalc; ++i) head[i] = head[i] * inv;
-  if (time) *time = t;
+  if (time) *time = (double)(float)t;
   return MSG_OK;
 }
 

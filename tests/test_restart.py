@@ -1,7 +1,7 @@
 """Checkpoint / resume through the reference's restart file (gfortran sequential
 unformatted: [int32 8][real(DP) time][int32 8] [int32 8n][n x real(DP) head*len_scal][int32 8n],
-Nonlinear_solution.f90:792-816; read back with head = value * (1/len_scal),
-Assign_calculation.f90:416-434)."""
+Nonlinear_solution.f90:792-816; read back with head = value * len_scal_inv, the reciprocal
+taken in single precision, Read_input.f90:1108, Assign_calculation.f90:416-434)."""
 import struct
 
 import numpy as np
@@ -26,7 +26,8 @@ def test_read_restart_written_like_gfortran(tmp_path):
     _fortran_file(p, 3600.0, vals)
     h, t = read_restart(p, 1000, ls)
     assert t == 3600.0
-    assert np.array_equal(h, vals * (1.0 / ls))
+    # value * len_scal_inv with the reciprocal taken in single precision, as assign_initv does
+    assert np.array_equal(h, vals * np.float64(np.float32(1.0) / np.float32(ls)))
     with pytest.raises(RuntimeError):
         read_restart(p, 999, ls)          # record length does not match the grid
     (tmp_path / "short.bin").write_bytes(p.read_bytes()[:100])
@@ -53,7 +54,7 @@ def test_write_restart_and_resume(tmp_path):
     assert np.array_equal(np.frombuffer(raw, "<f8", n, 20), h_dev * ls)
     h, t = read_restart(path, n, ls)
     assert t == 3600.0
-    assert np.max(np.abs(h - h_dev) / np.abs(h_dev)) <= 2.3e-16
+    assert np.array_equal(h, (h_dev * ls) * np.float64(np.float32(1.0) / np.float32(ls)))
     # resume: a new context started from the restart heads continues the run
     g2 = GpuSolver(p)
     g2.init_state(head=h)
