@@ -73,6 +73,87 @@ def read_field(path, shape):
     return raw.reshape(tuple(reversed(shape)))
 
 
+def ew(x, w=13, d=6):
+    """Fortran Ew.d output of a real (OUTFORM = "(E13.6)", Constval_module.f90:30): 0.ddd…
+    with d digits, exponent E+xx (or +xxx from 100 on), right-justified in w; w asterisks
+    when it does not fit."""
+    x = float(x)
+    if x != x:
+        s = "NaN"
+    elif x in (float("inf"), float("-inf")):
+        s = "-Infinity" if x < 0 else "Infinity"
+    elif x == 0.0:
+        s = "0." + "0" * d + "E+00"
+    else:
+        mant, ex = f"{abs(x):.{d - 1}E}".split("E")
+        e = int(ex) + 1
+        s = ("-" if x < 0 else "") + "0." + mant.replace(".", "") + (f"E{e:+03d}" if abs(e) <= 99 else f"{e:+04d}")
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+class MassBalance:
+    """The reference's whole-area mass-balance file (mass type 7, one region "whole area"):
+    write_mass_header (Write_output.f90:284-318) writes
+        <calc unit>,whole area
+        ,FLOW,STORAGE,RECHARGE,WELL,SURFACE,RIVER,LAKE,SEA,ALL
+    calc_cell_mas (Calc_output.f90:54-91) adds every time step's volumes, and at each output
+    time write_out_massf (Write_output.f90:498-538) scales them by len_scal**3 (a
+    single-precision product), calc_out_mass (Calc_output.f90:93-166) sums them and ALL,
+    and one line "time,FLOW,...,ALL" is written in E13.6, after which the sums restart.
+
+    Feed it msg_gpu_calc_mass's nine volumes after every accepted step (`add_step`) and
+    call `write(time_out)` at output times.  The ninth volume, free drainage through the
+    bottom (an extension without a reference column), is added into ALL only."""
+
+    COLUMNS = "FLOW,STORAGE,RECHARGE,WELL,SURFACE,RIVER,LAKE,SEA,ALL"
+
+    def __init__(self, path, cal_unit, len_scal):
+        self.path = path
+        lf = np.float32(len_scal)
+        self.cubic = float(lf * lf * lf)
+        self.acc = np.zeros(9)
+        with open(path, "w") as f:
+            f.write(f"{cal_unit.strip()},whole area\n,{self.COLUMNS}\n")
+
+    def add_step(self, volumes):
+        """One step's calc_mass volumes: storage, flow, recharge, well, surface, river,
+        lake, sea, drainage."""
+        v = np.asarray(volumes, dtype=np.float64)
+        if v.size != 9:
+            raise ValueError("add_step: nine volumes expected")
+        self.acc += v
+
+    def write(self, time_out):
+        sto, con, rec, wel, sur, riv, lak, sea, drn = self.acc * self.cubic
+        tot = sto + con + sea + wel + rec + sur + riv + lak + drn
+        vals = [con, sto, rec, wel, sur, riv, lak, sea, tot]
+        line = ew(np.float32(time_out)) + "".join("," + ew(v) for v in vals)
+        with open(self.path, "a") as f:
+            f.write(line + "\n")
+        self.acc[:] = 0.0
+        return line
+
+
+def read_mass(path):
+    """Rows of a mass-balance file (this writer's or the Fortran build's) as dicts of time
+    and the nine columns."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    cols = lines[1].split(",")[1:10]
+    rows = []
+    for s in lines[2:]:
+        v = [float(t.replace("E", "e")) if "E" in t else _fortran_real(t) for t in s.split(",")]
+        rows.append(dict(time=v[0], **{c: x for c, x in zip(cols, v[1:10])}))
+    return rows
+
+
+def _fortran_real(t):
+    """A real written without its E (exponent of three digits)."""
+    t = t.strip()
+    k = max(t.rfind("+"), t.rfind("-"))
+    return float(t[:k] + "e" + t[k:]) if k > 0 else float(t)
+
+
 def write_state(prefix, solver, time, len_scal):
     """Append the current head (unit len_scal), saturation (unit 1) and water table (unit
     len_scal, computed on the device) of `solver` to prefix + '_head.bin', '_srat.bin' and

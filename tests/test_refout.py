@@ -101,3 +101,36 @@ def test_input_field_round_trip(tmp_path):
     assert a.shape == (nz, ny, nx) and a[1, 0, 2] == v[nx * ny + 2]
     with pytest.raises(ValueError):
         refout.read_field(p, (nx, ny))
+
+
+@pytest.mark.parametrize("x,expect", [
+    (123.456, " 0.123456E+03"), (-0.001234567, "-0.123457E-02"), (0.0, " 0.000000E+00"),
+    (9.9999996, " 0.100000E+02"), (1e100, " 0.100000+101"), (-1e-120, "-0.100000-119"),
+])
+def test_ew_edit_descriptor(x, expect):
+    assert refout.ew(x) == expect
+
+
+def test_mass_balance_file(tmp_path):
+    p = tmp_path / "mass.csv"
+    ls = 10.0
+    mb = refout.MassBalance(p, "SEC", ls)
+    step = [-1.0e-3, 2.0e-3, 5.0e-4, 0.0, -1.0e-4, 0.0, 0.0, 3.0e-4, -1.5e-4]   # sto, flow, rech, ..., drain
+    mb.add_step(step)
+    mb.add_step(step)
+    line = mb.write(3600.0)
+    lines = p.read_text().splitlines()
+    assert lines[0] == "SEC,whole area"
+    assert lines[1] == ",FLOW,STORAGE,RECHARGE,WELL,SURFACE,RIVER,LAKE,SEA,ALL"
+    assert lines[2] == line and line.count(",") == 9 and all(len(t) == 13 for t in line.split(","))
+    (row,) = refout.read_mass(p)
+    c = 1000.0                                         # len_scal**3
+    assert row["time"] == 3600.0
+    assert row["FLOW"] == pytest.approx(2 * 2.0e-3 * c, rel=1e-6)
+    assert row["STORAGE"] == pytest.approx(2 * -1.0e-3 * c, rel=1e-6)
+    assert row["SEA"] == pytest.approx(2 * 3.0e-4 * c, rel=1e-6)
+    assert row["ALL"] == pytest.approx(2 * sum(step) * c, rel=1e-6)
+    mb.add_step(step)
+    mb.write(7200.0)                                   # the sums restart after each output
+    rows = refout.read_mass(p)
+    assert len(rows) == 2 and rows[1]["FLOW"] == pytest.approx(2.0e-3 * c, rel=1e-6)
