@@ -270,3 +270,19 @@ def test_time_step_heuristic():
         assert st["delt"] == min(dt * factor, prm["max_step"])
         assert st["current_t"] == float(np.float32(t + st["delt"]))
     assert len(seen) >= 2                     # the sequence exercises more than one branch
+
+
+def test_reference_amg_preconditioner_is_fine_dilu():
+    """Quirk Q1: loop_amg's post-smoother restarts from outx = inrhs (Linear_solution.f90:
+    495-740, :820), so with ref_quirks = 1 the reference's AMG preconditioner returns the
+    fine-level DILU solve, bit for bit."""
+    p = make_config("hetero", shape=(14, 12, 9), seed=4)
+    h = p.head0 + 0.003 * np.random.default_rng(2).standard_normal(p.ncalc)
+    out = []
+    for kw in (dict(precon_type=1, ref_quirks=1), dict(precon_type=0)):
+        o = Oracle(p, **kw)
+        o.init_state()
+        o.set_state(head_new=h, delt=1800.0)
+        o.set_system(*o.make_matvec())
+        out.append(o.precond(np.random.default_rng(7).standard_normal(p.ncalc)))
+    assert np.array_equal(out[0], out[1])
