@@ -8,7 +8,8 @@ what pins the restatement):
   an unsaturated column under recharge balances its fluxes term by term;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F;
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
-* the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern;
+* the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern, and the
+  reference's AMG preconditioner returns exactly the fine DILU solve (quirk Q1);
 * mass balance closes after a time step (Calc_function.f90:103-174);
 * the adaptive time step follows apply_heuri's three factors (Time_module.f90:1522-1543);
 * connectivity layout on a 2x2x3 box written out by hand (Set_condition.f90:1584-2026), and
