@@ -101,3 +101,12 @@ def test_null_context_is_an_argument_error():
     assert L.msg_gpu_water_table(None, out) == abi.MSG_ERR_ARG
     assert L.msg_gpu_calc_mass(None, out) == abi.MSG_ERR_ARG
     L.msg_gpu_destroy(None)                   # a no-op
+
+
+def test_missing_library_fails_loudly(monkeypatch):
+    """No CPU fallback: without the CUDA library every entry into the solver raises."""
+    from msg123_b200 import solver
+    monkeypatch.setattr(solver, "_lib", None)
+    monkeypatch.setattr(solver, "LIB_PATH", "/nonexistent/libmsg123gpu.so")
+    with pytest.raises(solver.MsgError, match="missing"):
+        solver.load_library()
