@@ -6,7 +6,8 @@ what pins the restatement):
 * hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101);
 * a unit-gradient saturated column between a ponded top and free drainage is steady, and
   an unsaturated column under recharge balances its fluxes term by term;
-* the finite-difference Jacobian of make_matrix agrees with a directional derivative of F;
+* the finite-difference Jacobian of make_matrix agrees with a directional derivative of F,
+  and calc_vecjacf is the Brown-Saad difference, recomputed bit for bit;
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern, and the
   reference's AMG preconditioner returns exactly the fine DILU solve (quirk Q1);
@@ -287,3 +288,27 @@ def test_reference_amg_preconditioner_is_fine_dilu():
         o.set_system(*o.make_matvec())
         out.append(o.precond(np.random.default_rng(7).standard_normal(p.ncalc)))
     assert np.array_equal(out[0], out[1])
+
+
+def test_vecjacf_is_brown_saad_difference():
+    """calc_vecjacf (Calc_function.f90:515-621): J v = -(F(x + eps v) - F(x)) / eps with
+    eps = sign(x.v) sqrt(eps_SP) max(|x.v|, |v|_1) / |v|^2, recomputed here from the
+    oracle's own residual with the same sequential sums -- bit for bit."""
+    import math
+    p = make_config("box", shape=(6, 5, 8))
+    o = Oracle(p)
+    o.init_state()
+    rng = np.random.default_rng(3)
+    x = p.head0 + 0.01 * rng.standard_normal(p.ncalc)
+    v = rng.standard_normal(p.ncalc)
+    l2_v = l2_x = l1_v = 0.0
+    for a, b in zip(x.tolist(), v.tolist()):
+        l2_v += b * b
+        l2_x += a * b
+        l1_v += abs(b)
+    sign = -1.0 if l2_x < 0.0 else 1.0
+    eps = sign * math.sqrt(float(np.finfo(np.float32).eps)) * max(abs(l2_x), l1_v) / l2_v
+    f1 = o.calc_func(x)
+    f2 = o.calc_func(x + eps * v)
+    want = -(f2 - f1) * (1.0 / eps)
+    assert np.array_equal(o.vecjacf(x, v), want)
