@@ -8,7 +8,8 @@ what pins the restatement):
   an unsaturated column under recharge balances its fluxes term by term;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F,
   and calc_vecjacf is the Brown-Saad difference, recomputed bit for bit;
-* BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493);
+* BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493), and its
+  iterates equal a second restatement of the Fortran recurrence bit for bit;
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern, and the
   reference's AMG preconditioner returns exactly the fine DILU solve (quirk Q1);
 * mass balance closes after a time step (Calc_function.f90:103-174);
@@ -312,3 +313,63 @@ def test_vecjacf_is_brown_saad_difference():
     f2 = o.calc_func(x + eps * v)
     want = -(f2 - f1) * (1.0 / eps)
     assert np.array_equal(o.vecjacf(x, v), want)
+
+
+def _seq_dot(a, b):
+    s = 0.0
+    for x, y in zip(a.tolist(), b.tolist()):
+        s += x * y
+    return s
+
+
+def _bicgs(o, b, bnorm, errtol, maxit):
+    """solve_bicgs (Linear_solution.f90:234-493) written out again from the Fortran, from
+    inx = 0 (so resi = b), with the oracle's own matvec and DILU apply and sequential sums."""
+    x = np.zeros_like(b)
+    resi = b.copy()
+    rs = resi.copy()
+    p = np.zeros_like(b)
+    v = np.zeros_like(b)
+    sk0, alpha, omega, rnorm = np.inf, 0.0, 1.0, 0.0
+    for it in range(1, maxit + 1):
+        sk = _seq_dot(resi, rs)
+        if it == 1:
+            p = resi.copy()
+        else:
+            beta = (sk / sk0) * (alpha / omega)
+            p = resi + beta * (p - omega * v)
+        z = o.precond(p)
+        v = o.matvec(z)
+        alpha = sk / _seq_dot(v, rs)
+        x = x + alpha * z
+        resi = resi - alpha * v
+        rnorm = _seq_dot(resi, resi)
+        if np.sqrt(rnorm / bnorm) <= errtol:
+            return x, rnorm, it
+        z = o.precond(resi)
+        t = o.matvec(z)
+        omega = _seq_dot(t, resi) / _seq_dot(t, t)
+        x = x + omega * z
+        resi = resi - omega * t
+        rnorm = _seq_dot(resi, resi)
+        if np.sqrt(rnorm / bnorm) <= errtol or it == maxit:
+            return x, rnorm, it
+        sk0 = sk
+    return x, rnorm, maxit
+
+
+@pytest.mark.parametrize("maxit", [1, 2, 4])
+def test_bicgstab_recurrence_restated_twice(maxit):
+    """The oracle's BiCGStab against a second restatement of the same Fortran: identical
+    iterates, residual norm and iteration count, bit for bit."""
+    p = make_config("hetero", shape=(10, 8, 6), seed=5, precon_type=0, maxinn_iter=maxit)
+    o = Oracle(p)
+    o.init_state()
+    o.set_state(head_new=p.head0 + 0.004 * np.random.default_rng(1).standard_normal(p.ncalc), delt=1800.0)
+    d, lu, b = o.make_matvec()
+    o.set_system(d, lu, b)
+    bnorm = _seq_dot(b, b)
+    xo, last, it, _ = o.solve_linalg(bnorm, 1e-30)
+    xp, rn, itp = _bicgs(o, b, bnorm, 1e-30, maxit)
+    assert it == itp == maxit
+    assert np.array_equal(xo, xp) and last == rn
