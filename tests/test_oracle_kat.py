@@ -8,6 +8,7 @@ what pins the restatement):
   an unsaturated column under recharge balances its fluxes term by term;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F,
   and calc_vecjacf is the Brown-Saad difference, recomputed bit for bit;
+* calc_matvec sums each CSR row in order (recomputed bit for bit);
 * BiCGStab + DILU solves the assembled system (Linear_solution.f90:234-493), and its
   iterates equal a second restatement of the Fortran recurrence bit for bit;
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern, and the
@@ -373,3 +374,24 @@ def test_bicgstab_recurrence_restated_twice(maxit):
     xp, rn, itp = _bicgs(o, b, bnorm, 1e-30, maxit)
     assert it == itp == maxit
     assert np.array_equal(xo, xp) and last == rn
+
+
+def test_matvec_row_order():
+    """calc_matvec (Linear_solution.f90:917-951): y_i = d_i x_i, then + lumat_k x_j over the
+    row's CSR entries in order -- recomputed from the exported connectivity, bit for bit."""
+    p = make_config("hetero", shape=(7, 6, 5), seed=8, precon_type=0)
+    o = Oracle(p)
+    o.init_state()
+    o.set_state(head_new=p.head0 + 0.004 * np.random.default_rng(4).standard_normal(p.ncalc), delt=1800.0)
+    d, lu, b = o.make_matvec()
+    o.set_system(d, lu, b)
+    c = o.connect()
+    x = np.random.default_rng(6).standard_normal(p.ncalc)
+    y = np.empty(p.ncalc)
+    xl, dl, ll = x.tolist(), d.tolist(), lu.tolist()
+    for i in range(p.ncalc):
+        t = dl[i] * xl[i]
+        for k in range(c["offind"][i], c["offind"][i + 1]):
+            t = t + ll[k] * xl[c["offrow"][k] - 1]
+        y[i] = t
+    assert np.array_equal(o.matvec(x), y)
