@@ -2,7 +2,8 @@
 golden vectors, and no Fortran compiler exists here, so these analytic checks are
 what pins the restatement):
 
-* van Genuchten / Mualem closed forms at chosen pressure heads (Calc_parameter.f90:15-77);
+* van Genuchten / Mualem closed forms at chosen pressure heads (Calc_parameter.f90:15-77),
+  and a second restatement with the C library's pow, bit for bit, in both kr forms;
 * hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101);
 * a unit-gradient saturated column between a ponded top and free drainage is steady, and
   an unsaturated column under recharge balances its fluxes term by term;
@@ -438,3 +439,34 @@ def test_dilu_and_ilu_solve_restated():
         x[i] = x[i] - t / d[i]
     assert np.array_equal(o.solve_ilu(np.array(d), rhs), np.array(x))
     assert np.array_equal(o.precond(rhs), np.array(x))
+
+
+@pytest.mark.parametrize("vg_form", [0, 1])
+def test_srat_rperm_restated(vg_form):
+    """calc_srat_rperm (Calc_parameter.f90:15-77) written out again with the same operation
+    order and the C library's pow (Python's math.pow; numpy's vectorised power differs in
+    the last bit), theta_s - theta_r a single-precision difference as the real(SP) parameters
+    give it; S and kr agree bit for bit.  vg_form 1 is the library's two-pow form of kr."""
+    import math
+    p = make_config("hetero", shape=(8, 7, 6), seed=17, vg_form=vg_form)
+    o = Oracle(p)
+    rng = np.random.default_rng(11)
+    h = p.cell_top + rng.uniform(-3.0, 0.3, p.ncalc)
+    for pert in (0.0, 1.19e-9):
+        s, kr, ss = o.srat_rperm(h, pert)
+        for i in range(p.ncalc):
+            ph = float(h[i]) - float(p.cell_top[i]) + pert
+            if ph >= 0.0:
+                assert s[i] == 1.0 and kr[i] == 1.0 and ss[i] == float(p.ss[i])
+                continue
+            n = float(p.retn[i])
+            m = 1.0 - 1.0 / n
+            a = abs(ph * float(p.reta[i]))
+            beta = math.pow(a, n)
+            se = math.pow(1.0 + beta, -m)
+            theta = float(p.resi[i]) + float(p.poro[i] - p.resi[i]) * se
+            if vg_form == 0:
+                t = 1.0 - math.pow(1.0 - math.pow(se, 1.0 / m), m)
+            else:
+                t = 1.0 - (0.0 if beta == 0.0 or se == 0.0 else se * (beta / a))
+            assert s[i] == theta / float(p.poro[i]) and kr[i] == math.sqrt(se) * (t * t) and ss[i] == 0.0
