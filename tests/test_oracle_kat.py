@@ -4,7 +4,9 @@ what pins the restatement):
 
 * van Genuchten / Mualem closed forms at chosen pressure heads (Calc_parameter.f90:15-77),
   and a second restatement with the C library's pow, bit for bit, in both kr forms;
-* hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101);
+* hydrostatic equilibrium gives F == 0 exactly (Calc_function.f90:24-101), and the residual
+  equals a second term-by-term restatement (storage, upwind flow, recharge, surface, sea,
+  free drainage) bit for bit;
 * a unit-gradient saturated column between a ponded top and free drainage is steady, and
   an unsaturated column under recharge balances its fluxes term by term;
 * the finite-difference Jacobian of make_matrix agrees with a directional derivative of F,
@@ -470,3 +472,95 @@ def test_srat_rperm_restated(vg_form):
             else:
                 t = 1.0 - (0.0 if beta == 0.0 or se == 0.0 else se * (beta / a))
             assert s[i] == theta / float(p.poro[i]) and kr[i] == math.sqrt(se) * (t * t) and ss[i] == 0.0
+
+
+def _vg(p, h):
+    """(S, kr, alp_ss) per cell as calc_srat_rperm computes them (reference kr form)."""
+    import math
+    S, kr, alp = [], [], []
+    for i in range(p.ncalc):
+        ph = float(h[i]) - float(p.cell_top[i]) + 0.0
+        if ph < 0.0:
+            n = float(p.retn[i])
+            m = 1.0 - 1.0 / n
+            beta = math.pow(abs(ph * float(p.reta[i])), n)
+            se = math.pow(1.0 + beta, -m)
+            S.append((float(p.resi[i]) + float(p.poro[i] - p.resi[i]) * se) / float(p.poro[i]))
+            t = 1.0 - math.pow(1.0 - math.pow(se, 1.0 / m), m)
+            kr.append(math.sqrt(se) * (t * t))
+            alp.append(0.0)
+        else:
+            S.append(1.0)
+            kr.append(1.0)
+            alp.append(float(p.ss[i]))
+    return S, kr, alp
+
+
+@pytest.mark.parametrize("name,kw", [("box", dict(shape=(5, 4, 6))), ("hetero", dict(shape=(6, 5, 4), seed=23))])
+def test_calc_func_restated(name, kw):
+    """calc_func (Calc_function.f90:24-101) written out again term by term -- func_stochn
+    (:176-210), func_connflow with upwind kr (:212-254, Calc_parameter.f90:107-125),
+    func_rechterm (:256-275), func_surfterm (:304-391), func_sealterm (:475-513), summed in the
+    reference's order, plus the free-drainage extension last -- on a state with ponded,
+    unsaturated and saturated top cells; the oracle's residual agrees bit for bit."""
+    import math
+    p = make_config(name, **kw)
+    N, S = p.ncalc, p.ncals
+    rng = np.random.default_rng(31)
+    h_old = p.head0 + 0.02 * rng.standard_normal(N)
+    h = h_old + 0.01 * rng.standard_normal(N)
+    h[: S // 3] = p.surf_top[: S // 3] + 0.003 / p.params["len_scal"]     # some ponded top cells
+    sh = p.surf_top + rng.uniform(-0.01, 0.01, S) / p.params["len_scal"]
+    o = Oracle(p)
+    o.init_state()
+    s_old = o.srat_rperm(h_old)[0]
+    o.set_state(head_new=h, head_old=h_old, srat_old=s_old, surf_head=sh, delt=1800.0)
+    o.set_recharge(p.rech)
+    f = o.calc_func(h)
+
+    Sn, kr, alp = _vg(p, h)
+    c = o.connect()
+    dis, far = p.dis2face.reshape(6, N), p.face_area.reshape(6, N)
+    delt_inv = 1.0 / 1800.0
+    out = []
+    for i in range(N):
+        ch1 = alp[i] * float(s_old[i]) * float(h_old[i])
+        ch2 = alp[i] * Sn[i] * float(h[i])
+        ch = (ch2 - ch1) + float(p.poro[i]) * (Sn[i] - float(s_old[i]))
+        stof = -ch * delt_inv * float(p.cell_vol[i])
+        conf = 0.0
+        for k in range(c["offind"][i], c["offind"][i + 1]):
+            j = c["offrow"][k] - 1
+            dh = float(h[j]) - float(h[i])
+            relat = kr[i] if -dh >= 0.0 else kr[j]
+            conf = conf + float(c["hydf"][k]) * relat * float(c["abyd"][k]) * dh
+        fs, seaf = 0.0, 0.0
+        if i < S:
+            x, sh_i = float(h[i]), float(sh[i])
+            top, bot, reli, parm = (float(p.surf_top[i]), float(p.surf_bott[i]), float(p.surf_reli[i]),
+                                    float(p.surf_parm[i]))
+            rati = 1.0
+            if x >= top:
+                delh = sh_i - x if sh_i > top else top - x
+            elif x >= bot:
+                delh = sh_i - x if sh_i > bot else bot - x
+                if reli != 0.0:
+                    rati = math.pow(min((x - bot) / reli, 1.0), parm)
+            elif sh_i > bot:
+                delh = sh_i - bot
+                if reli != 0.0:
+                    rati = math.pow(min((sh_i - bot) / reli, 1.0), parm)
+            else:
+                delh = 0.0
+            # a top cell under a sea layer meets the sea through its up face and has no
+            # surface face: its surface conductance and area stay zero (set_connect)
+            hyd_s, a_s = (0.0, 0.0) if p.sea_top else (float(p.ksz[i]), far[0, i])
+            surf = hyd_s * (a_s / dis[0, i]) * delh * kr[i] * rati
+            fs = float(p.rech[i]) + surf + 0.0 + 0.0
+            if p.sea_top:
+                seaf = 0.0 + float(p.ksz[i]) * kr[i] * (far[0, i] / dis[0, i]) * (float(p.sea_head[i]) - x)
+        fi = fs + stof + conf + 0.0 + seaf
+        if p.free_drainage and i >= N - S:
+            fi = fi + (-((float(p.ksz[i]) * far[5, i]) * kr[i]))
+        out.append(fi)
+    assert np.array_equal(f, np.array(out))
