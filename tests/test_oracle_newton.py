@@ -1,0 +1,231 @@
+"""calc_numsol (Nonlinear_solution.f90:33-294) with set_backtr (:386-412), set_eater
+(:414-439), run_backtr (:441-631) and check_abserrmax (Check_simulation.f90:37-91),
+written out again in Python from the Fortran and driven by the oracle's own make_matvec,
+solve_linalg, calc_func and calc_vecjacf (each pinned separately in test_oracle_kat.py):
+the oracle's Newton solve must land on the same heads, bit for bit, with the same Newton,
+Krylov and backtracking counts.  This pins the Newton controller -- the inexact-Newton
+forcing, the step-length cap and the cubic/quadratic line search -- against the source.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from msg123_b200.config import make_config
+from oracle.oracle import Oracle
+
+VARMAX, XMAX = 1.0e3, 1.0e4
+MACHI_EPS = float(np.finfo(np.float32).eps)
+
+
+def _dot(a, b):
+    s = 0.0
+    for x, y in zip(a.tolist(), b.tolist()):
+        s += x * y
+    return s
+
+
+def _maxnum(a, b):
+    """MAX of two reals when one may be NaN: the other one (IEEE 754 maxNum, what gfortran's
+    MAX and C's fmax return)."""
+    if a != a:
+        return b
+    if b != b:
+        return a
+    return max(a, b)
+
+
+def _abserrmax(x_new, x_pre):
+    ach = aval = bch = bval = 0.0
+    nun = 0
+    for i, (a, b) in enumerate(zip(x_new.tolist(), x_pre.tolist())):
+        d = a - b
+        if abs(d) >= ach:
+            bch, ach, nun = d, abs(d), i + 1
+        if abs(a) >= aval:
+            aval, bval = abs(a), a
+    return bch, bval, nun
+
+
+class _Newton:
+    def __init__(self, o, prm):
+        self.o, self.prm = o, prm
+
+    def func_l2(self, h):
+        f = self.o.calc_func(h)
+        return _dot(f, f)
+
+    def run_backtr(self, h_pre, dh, h_new, rhs, l2_pre, l2_jnorm, maxstep):
+        o = self.o
+        lam, lam2, maxpnorm, lam_length = 1.0, 1.0, 1.0, 1.0
+        f = o.calc_func(h_new)
+        l2_pnorm = _dot(dh, dh)
+        jac = o.vecjacf(h_pre, dh)
+        sq = math.sqrt(l2_pnorm)
+        if sq > maxstep:
+            maxpnorm = maxstep / sq
+            dh = dh * maxpnorm
+            sq = maxstep
+        step_len = sq
+        l2_new = _dot(f, f)
+        slope = _dot(rhs, jac) * maxpnorm
+        for a, b in zip(dh.tolist(), h_new.tolist()):
+            if b != 0.0:
+                t = abs(a) / abs(b)
+                if t > lam_length:
+                    lam_length = t
+        l2_jnorm = l2_jnorm * maxpnorm * maxpnorm
+        lam_min = math.pow(MACHI_EPS, 2.0 / 3.0) / lam_length
+        alpha_cond = 0.5 * l2_pre + 1.0e-4 * lam * slope
+        back_iter = beta_iter = 0
+        l2_new2 = 0.0
+        h = h_new
+        while not (0.5 * l2_new <= alpha_cond):
+            back_iter += 1
+            h = h_pre + lam * dh
+            l2_new = self.func_l2(h)
+            if lam == 1.0:
+                tl = -slope / (2.0 * (0.5 * l2_new - 0.5 * l2_pre - slope))
+            else:
+                r1 = 0.5 * l2_new - 0.5 * l2_pre - lam * slope
+                r2 = l2_new2 - 0.5 * l2_pre - lam2 * slope
+                li, l2i, dl = 1.0 / (lam ** 2), 1.0 / (lam2 ** 2), 1.0 / (lam - lam2)
+                av = (r1 * li - r2 * l2i) * dl
+                bv = (-lam2 * r1 * li + lam * r2 * l2i) * dl
+                if av == 0:
+                    tl = -slope / (2.0 * bv)
+                else:
+                    root = bv * bv - 3.0 * av * slope
+                    if root < 0.0:
+                        tl = 0.5 * lam
+                    elif bv <= 0.0:
+                        tl = (-bv + math.sqrt(root)) / (3.0 * av)
+                    else:
+                        tl = -slope / (bv + math.sqrt(root))
+                    if tl > 0.5 * lam:
+                        tl = 0.5 * lam
+            lam2, l2_new2 = lam, 0.5 * l2_new
+            lam = max(tl, 0.1 * lam)
+            if lam < lam_min:
+                return h, l2_new, lam, slope, l2_jnorm, 1, back_iter
+            alpha_cond = 0.5 * l2_pre + 1.0e-4 * lam * slope
+        alpha_cond = 0.5 * l2_pre + 1.0e-4 * lam * slope
+        beta_cond = 0.5 * l2_pre + 0.9 * lam * slope
+        if 0.5 * l2_new < beta_cond:
+            if lam == 1.0 and sq < step_len:
+                lam_max = step_len / sq
+                while not (0.5 * l2_new > alpha_cond or 0.5 * l2_new >= beta_cond or lam >= lam_max):
+                    lam2, l2_new2, lam = lam, 0.5 * l2_new, min(2.0 * lam, lam_max)
+                    h = h_pre + lam * dh
+                    l2_new = self.func_l2(h)
+                    alpha_cond = 0.5 * l2_pre + 1.0e-4 * lam * slope
+                    beta_cond = 0.5 * l2_pre + 0.9 * lam * slope
+            if lam < 1.0 or (lam > 1.0 and 0.5 * l2_new > alpha_cond):
+                lam_base, lam_diff = min(lam, lam2), abs(lam2 - lam)
+                while not (0.5 * l2_new <= alpha_cond and (0.5 * l2_new >= beta_cond or lam_diff <= lam_min)):
+                    incr = 0.5 * lam_diff
+                    lam = lam_base + incr
+                    h = h_pre + lam * dh
+                    l2_new = self.func_l2(h)
+                    alpha_cond = 0.5 * l2_pre + 1.0e-4 * lam * slope
+                    beta_cond = 0.5 * l2_pre + 0.9 * lam * slope
+                    if 0.5 * l2_new > alpha_cond:
+                        lam_diff = incr
+                    elif 0.5 * l2_new < beta_cond:
+                        lam_base, lam_diff = lam, lam_diff - incr
+                    if lam_diff == 0.0:
+                        break
+                if 0.5 * l2_new < beta_cond:
+                    h = h_pre + lam_base * dh
+                    l2_new = self.func_l2(h)
+                    beta_iter += 1
+                if beta_iter == 10:
+                    return h, l2_new, lam, slope, l2_jnorm, 1, back_iter
+        return h, l2_new, lam, slope, l2_jnorm, 0, back_iter
+
+    def solve(self, h):
+        o, prm = self.o, self.prm
+        ls = prm["len_scal"]
+        maxstep = max(math.sqrt(_dot(h, h)) * VARMAX, 1.0)          # set_backtr
+        inner = backs = 0
+        status, l2_new, eta = None, 0.0, 0.5
+        for out_iter in range(1, prm["maxout_iter"] + 1):
+            if out_iter > 1:
+                l2_pre = l2_new
+            o.set_state(head_new=h)
+            _, _, rhs = o.make_matvec()
+            if out_iter == 1:
+                l2_new = _dot(rhs, rhs)
+                l2_pre, eta = l2_new, 0.5
+            h_pre = h
+            errtol = prm["lin_tol"] if prm["lin_tol"] > 0 else eta
+            dh, l2_jnorm, it, conv = o.solve_linalg(l2_pre, errtol)
+            inner += it
+            h = h_pre + dh
+            maxvar, maxunk, _ = _abserrmax(h, h_pre)
+            check, maxunk = abs(maxvar) * ls, abs(maxunk) * ls
+            crit = prm["criteria"] * maxunk if prm["criteria_rel"] else prm["criteria"]
+            conv_flag, back_flag = conv, 0
+            if conv_flag != 0:
+                conv_flag = 1 if (check <= crit and maxunk < XMAX) else 0
+            if conv_flag != 1:
+                h, l2_new, lam, slope, l2_jnorm, back_flag, bi = self.run_backtr(
+                    h_pre, dh, h, rhs, l2_pre, l2_jnorm, maxstep)
+                backs += bi
+                maxvar, maxunk, _ = _abserrmax(h, h_pre)
+                check, maxunk = abs(maxvar) * ls, abs(maxunk) * ls
+                crit = prm["criteria"] * maxunk if prm["criteria_rel"] else prm["criteria"]
+                if check >= VARMAX or maxunk >= XMAX:
+                    back_flag = 1
+                elif check <= crit and maxunk < XMAX:
+                    conv_flag = 1
+                if conv_flag != 1 and back_flag != 1:                   # set_eater
+                    eta_safe = math.pow(eta, (1.0 + math.sqrt(5.0)) / 2.0)
+                    m1 = 1.0 - lam
+                    q = m1 * m1 * l2_pre + 2.0 * lam * m1 * slope + lam * lam * l2_jnorm
+                    lin = math.sqrt(q) if q >= 0.0 else math.nan      # IEEE sqrt of a negative
+                    eta = abs(math.sqrt(l2_new) - lin) / math.sqrt(l2_pre)
+                    if eta_safe < 0.1:
+                        eta_safe = 0.0
+                    eta = min(_maxnum(_maxnum(eta, eta_safe), 1.0e-4), 0.9)
+            l2_new = _dot(*(2 * [o.calc_func(h)]))
+            if conv_flag == 1:
+                status = 0
+            elif back_flag == 1:
+                status = 3
+            elif out_iter == prm["maxout_iter"]:
+                status = 1
+            elif abs(maxvar * ls) >= VARMAX or maxunk >= XMAX:
+                status = 4
+            if status is not None:
+                return h, status, out_iter, inner, backs, maxvar * ls, l2_new
+        raise AssertionError("unreachable")
+
+
+def _case(name, kw, amp, seed):
+    p = make_config(name, precon_type=0, **kw)
+    h0 = p.head0 + amp * np.random.default_rng(seed).standard_normal(p.ncalc) / p.params["len_scal"]
+    pair = []
+    for _ in range(2):
+        o = Oracle(p)
+        o.init_state(head=h0)
+        pair.append(o)
+    return p, pair
+
+
+@pytest.mark.parametrize("name,kw,amp,seed", [
+    ("box", dict(shape=(6, 5, 10)), 0.0, 0),
+    ("hetero", dict(shape=(10, 8, 6), seed=3), 0.0, 0),
+    ("hetero", dict(shape=(10, 8, 6), seed=3, maxinn_iter=3), 0.3, 1),   # inexact solves, rough start
+    ("hetero", dict(shape=(10, 8, 6), seed=3, maxinn_iter=2), 1.0, 2),   # 18 backtracks, Newton cap
+    ("hetero", dict(shape=(10, 8, 6), seed=7, maxinn_iter=1), 2.0, 4),   # 24 backtracks, Newton cap
+])
+def test_newton_controller_restated(name, kw, amp, seed):
+    p, (o1, o2) = _case(name, kw, amp, seed)
+    rc, st = o1.calc_numsol()
+    h1 = o1.get_state()["head_new"]
+    h2, status, out_iter, inner, backs, maxvar, l2 = _Newton(o2, dict(p.params, precon_type=0, **kw)).solve(
+        o2.get_state()["head_new"].copy())
+    assert (rc, st["out_iter"], st["inner_total"], st["back_total"]) == (status, out_iter, inner, backs)
+    assert np.array_equal(h1, h2)
+    assert st["maxvar"] == maxvar and st["l2_new"] == l2
