@@ -20,6 +20,8 @@ what pins the restatement):
   reference's AMG preconditioner returns exactly the fine DILU solve (quirk Q1);
 * mass balance closes after a time step (Calc_function.f90:103-174);
 * the adaptive time step follows apply_heuri's three factors (Time_module.f90:1522-1543);
+* the AMG strength filter and smoothed prolongation restated from the Fortran (P bit for
+  bit) and the coarse operator equal to P^T A P;
 * connectivity layout on a 2x2x3 box written out by hand (Set_condition.f90:1584-2026), and
   every face conductance equal to the distance-weighted harmonic mean of the two cells' K_s.
 """
@@ -635,3 +637,63 @@ def test_make_matrix_restated(name, kw):
         d_ref.append(di)
     assert np.array_equal(lu, lu_ref)
     assert np.array_equal(dm, np.array(d_ref))
+
+
+def test_amg_prolongation_and_galerkin():
+    """The AMG built by the oracle, level 1 -> 2, against the reference's formulas:
+    make_grapfilt's strength filter (Make_amg_matrix.f90:66-111: a_ij strong when
+    a_ij^2 > |d_i d_j theta^2| and d_i d_j a_ij > 0, weak entries lumped into the filtered
+    diagonal) and make_prolomat's smoothed prolongation (:224-371: columns in order of first
+    appearance among the strong neighbours' aggregates, then the row's own; values
+    -sum a_ij * omega / d~_i, plus 1 - omega on the own aggregate), restated from the
+    Fortran with the oracle's aggregates -- P bit for bit; and the coarse operator equal
+    to P^T A P (scipy) to rounding."""
+    import scipy.sparse as sp
+    p = make_config("hetero", shape=(12, 10, 8), seed=4, precon_type=1, ref_quirks=0, amg_coarse_max=50)
+    o = Oracle(p)
+    o.init_state()
+    o.set_state(head_new=p.head0 + 0.003 * np.random.default_rng(2).standard_normal(p.ncalc), delt=1800.0)
+    o.set_system(*o.make_matvec())
+    lv = o.amg_levels()
+    assert len(lv) >= 2
+    l0, l1 = lv[0], lv[1]
+    d, lu, off, col, agg = (l0["dmat"].tolist(), l0["lumat"].tolist(), l0["offind"].tolist(),
+                            l0["offrow"].tolist(), l1["agg"].tolist())
+    th = float(np.float32(p.params["amg_theta"]))
+    th2, om = th * th, float(np.float32(p.params["jac_omega"]))
+    pind, pcol, pval = [0], [], []
+    for i in range(l0["n"]):
+        td, strong = d[i], []
+        for k in range(off[i], off[i + 1]):
+            dd = d[i] * d[col[k]]
+            if lu[k] * lu[k] > abs(dd * th2) and dd * lu[k] > 0.0:
+                strong.append(k)
+            else:
+                td = td + lu[k]
+        ags = []
+        for k in strong:
+            a = agg[col[k]]
+            if a >= 0 and a not in ags:
+                ags.append(a)
+        if agg[i] >= 0 and agg[i] not in ags:
+            ags.append(agg[i])
+        vals = [0.0] * len(ags)
+        for k in strong:
+            a = agg[col[k]]
+            if a >= 0:
+                vals[ags.index(a)] = vals[ags.index(a)] - lu[k]
+        vals = [v * om / td for v in vals]
+        if agg[i] >= 0:
+            q = ags.index(agg[i])
+            vals[q] = vals[q] + 1.0 - om
+        pcol += ags
+        pval += vals
+        pind.append(len(pcol))
+    assert l1["pindex"].tolist() == pind and l1["poffrow"].tolist() == pcol
+    assert np.array_equal(l1["pval"], np.array(pval))
+    n0, n1 = l0["n"], l1["n"]
+    A = sp.csr_matrix((l0["lumat"], l0["offrow"], l0["offind"]), shape=(n0, n0)) + sp.diags(l0["dmat"])
+    P = sp.csr_matrix((l1["pval"], l1["poffrow"], l1["pindex"]), shape=(n0, n1))
+    Ac = (P.T @ A @ P).toarray()
+    Ao = sp.csr_matrix((l1["lumat"], l1["offrow"], l1["offind"]), shape=(n1, n1)).toarray() + np.diag(l1["dmat"])
+    assert np.max(np.abs(Ao - Ac)) <= 1e-12 * np.max(np.abs(Ac))
