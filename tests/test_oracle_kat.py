@@ -18,7 +18,8 @@ what pins the restatement):
 * the DILU diagonal and the ILU sweeps equal a second restatement bit for bit;
 * the DILU diagonal equals the ILU(0) pivots of a dense LU restricted to the pattern, and the
   reference's AMG preconditioner returns exactly the fine DILU solve (quirk Q1);
-* mass balance closes after a time step (Calc_function.f90:103-174);
+* mass balance closes after a time step (Calc_function.f90:103-174), and calc_mass's nine
+  volumes equal a second restatement bit for bit;
 * the adaptive time step follows apply_heuri's three factors (Time_module.f90:1522-1543);
 * the AMG strength filter and smoothed prolongation restated from the Fortran (P bit for
   bit) and the coarse operator equal to P^T A P;
@@ -697,3 +698,69 @@ def test_amg_prolongation_and_galerkin():
     Ac = (P.T @ A @ P).toarray()
     Ao = sp.csr_matrix((l1["lumat"], l1["offrow"], l1["offind"]), shape=(n1, n1)).toarray() + np.diag(l1["dmat"])
     assert np.max(np.abs(Ao - Ac)) <= 1e-12 * np.max(np.abs(Ac))
+
+
+@pytest.mark.parametrize("name,kw", [("box", dict(shape=(5, 4, 6))), ("hetero", dict(shape=(6, 5, 4), seed=23))])
+def test_calc_mass_restated(name, kw):
+    """calc_mass (Calc_function.f90:103-174, sfla = 0) written out again: storage change with
+    the old level's storage coefficient, upwind flow, recharge, surface (against the surface
+    heads of the previous step), sea and the free-drainage extension, each times delt and
+    summed over cells in order -- the oracle's nine volumes agree bit for bit."""
+    import math
+    p = make_config(name, **kw)
+    N, S = p.ncalc, p.ncals
+    rng = np.random.default_rng(41)
+    h_old = p.head0 + 0.02 * rng.standard_normal(N)
+    h = h_old + 0.01 * rng.standard_normal(N)
+    h[: S // 3] = p.surf_top[: S // 3] + 0.003 / p.params["len_scal"]
+    sh = p.surf_top + rng.uniform(-0.01, 0.01, S) / p.params["len_scal"]
+    delt = 1800.0
+    o = Oracle(p)
+    o.init_state()
+    s_old = o.srat_rperm(h_old)[0]
+    o.set_state(head_new=h, head_old=h_old, srat_old=s_old, surf_head=sh, delt=delt)
+    o.set_recharge(p.rech)
+    got = o.calc_mass()
+
+    _, _, alp_o = _vg(p, h_old)
+    sn, kr, alp_n = _vg(p, h)
+    c = o.connect()
+    dis, far = p.dis2face.reshape(6, N), p.face_area.reshape(6, N)
+    acc = [0.0] * 9
+    for i in range(N):
+        ch1 = alp_o[i] * float(s_old[i]) * float(h_old[i])
+        ch2 = alp_n[i] * sn[i] * float(h[i])
+        ch = (ch2 - ch1) + float(p.poro[i]) * (sn[i] - float(s_old[i]))
+        acc[0] += -ch * (1.0 / delt) * float(p.cell_vol[i]) * delt
+        cf = 0.0
+        for k in range(c["offind"][i], c["offind"][i + 1]):
+            j = c["offrow"][k] - 1
+            dh = float(h[j]) - float(h[i])
+            cf = cf + float(c["hydf"][k]) * (kr[i] if -dh >= 0.0 else kr[j]) * float(c["abyd"][k]) * dh
+        acc[1] += cf * delt
+        if p.free_drainage and i >= N - S:
+            acc[8] += -((float(p.ksz[i]) * far[5, i]) * kr[i]) * delt
+    for s in range(S):
+        x, shs = float(h[s]), float(sh[s])
+        top, bot, reli, parm = float(p.surf_top[s]), float(p.surf_bott[s]), float(p.surf_reli[s]), float(p.surf_parm[s])
+        rati = 1.0
+        if x >= top:
+            delh = shs - x if shs > top else top - x
+        elif x >= bot:
+            delh = shs - x if shs > bot else bot - x
+            if reli != 0.0:
+                rati = math.pow(min((x - bot) / reli, 1.0), parm)
+        elif shs > bot:
+            delh = shs - bot
+            if reli != 0.0:
+                rati = math.pow(min((shs - bot) / reli, 1.0), parm)
+        else:
+            delh = 0.0
+        hyd_s, a_s = (0.0, 0.0) if p.sea_top else (float(p.ksz[s]), far[0, s])
+        acc[2] += float(p.rech[s]) * delt
+        acc[4] += hyd_s * (a_s / dis[0, s]) * delh * kr[s] * rati * delt
+    if p.sea_top:
+        for s in range(S):
+            dh = float(p.sea_head[s]) - float(h[s])
+            acc[7] += float(p.ksz[s]) * kr[s] * (far[0, s] / dis[0, s]) * dh * delt
+    assert np.array_equal(got, np.array(acc))
