@@ -5,6 +5,8 @@ solve_linalg, calc_func and calc_vecjacf (each pinned separately in test_oracle_
 the oracle's Newton solve must land on the same heads, bit for bit, with the same Newton,
 Krylov and backtracking counts.  This pins the Newton controller -- the inexact-Newton
 forcing, the step-length cap and the cubic/quadratic line search -- against the source.
+The time loop around it (accept, reject and roll back, dt control, the real(SP) clock) is
+restated the same way.
 """
 import math
 
@@ -229,3 +231,77 @@ def test_newton_controller_restated(name, kw, amp, seed):
     assert (rc, st["out_iter"], st["inner_total"], st["back_total"]) == (status, out_iter, inner, backs)
     assert np.array_equal(h1, h2)
     assert st["maxvar"] == maxvar and st["l2_new"] == l2
+
+
+def _time_loop(o, p, nsteps, rech_until, rech_after):
+    """update_tstep / calc_nextst / apply_heuri (Time_module.f90:34-273, :1522-1543) written
+    out again around the oracle's calc_numsol: accept -> shift the time levels and grow dt by
+    inc_fact or the Newton-count heuristic (capped at max_step); reject -> roll back, step the
+    real(SP) clock back and halve dt; the recharge switches at rech_until, where a step is
+    cut to land on it (the library's set_delt alignment), and dt below 1e-20 stops."""
+    prm = p.params
+    f32 = lambda x: float(np.float32(x))
+    st = o.get_state()
+    hn, ho, so, sh = st["head_new"], st["head_old"], st["srat_old"], st["surf_head"]
+    ho2, surf_old = ho.copy(), sh.copy()
+    delt, t, nts, d_old1, conv, last_out = prm["ini_step"], 0.0, 0, 0.0, -1, 0
+    R = dict(accepted=0, rejected=0, newton_total=0, krylov_total=0, back_total=0)
+    incr, decr = int(prm["maxout_iter"] * 0.4), int(prm["maxout_iter"] * 0.8)
+    while R["accepted"] < nsteps:
+        if conv == 1:
+            if nts == 0:
+                d_old1 = delt
+            nts += 1
+            d_old1 = delt
+            if prm["sim_type"] == 0:
+                delt = delt * prm["inc_fact"]
+            else:
+                delt = d_old1 * (1.2 if last_out <= incr else (1.0 if last_out <= decr else 0.8))
+                if delt > prm["max_step"]:
+                    delt = prm["max_step"]
+            ho2, ho, so, surf_old = ho, hn, sn, sh
+        elif conv == 0:
+            t = f32(t - f32(delt))
+            delt = delt * 0.5
+            hn, sh = ho, surf_old
+            R["rejected"] += 1
+        if t < rech_until and t + delt > rech_until:
+            delt = rech_until - t
+        if t + delt > prm["end_time"]:
+            delt = prm["end_time"] - t
+        if delt < 1.0e-20:
+            return 5, R, hn, t, delt
+        o.set_recharge(p.rech * (1.0 if t < rech_until else rech_after))
+        t = f32(t + f32(delt))
+        o.set_state(head_new=hn, head_old=ho, srat_old=so, surf_head=sh, delt=delt)
+        rc, s = o.calc_numsol()
+        for k in ("newton_total", "krylov_total", "back_total"):
+            R[k] += s[{"newton_total": "out_iter", "krylov_total": "inner_total", "back_total": "back_total"}[k]]
+        last_out = s["out_iter"]
+        conv = 1 if rc == 0 else 0
+        g = o.get_state()
+        hn, sn, sh = g["head_new"], g["srat_new"], g["surf_head"]
+        if conv:
+            R["accepted"] += 1
+            if t >= prm["end_time"]:
+                break
+    return 0, R, hn, t, delt
+
+
+@pytest.mark.parametrize("name,kw,nsteps,rech_until", [
+    ("box", dict(shape=(6, 5, 8), maxout_iter=2), 3, 1.0e30),             # Newton cap: rejections, dt halving
+    ("hetero", dict(shape=(10, 8, 6), seed=3), 6, 2000.0),                 # heuristic dt, rain stops mid-run
+])
+def test_time_loop_restated(name, kw, nsteps, rech_until):
+    p = make_config(name, precon_type=0, **kw)
+    o1, o2 = Oracle(p), Oracle(p)
+    for o in (o1, o2):
+        o.init_state()
+        o.set_recharge(p.rech)
+    rc1, r1 = o1.advance(nsteps=nsteps, rech_until=rech_until, rech_after=0.0)
+    rc2, r2, h2, t2, d2 = _time_loop(o2, p, nsteps, rech_until, 0.0)
+    assert rc1 == rc2 == 0
+    for k in ("accepted", "rejected", "newton_total", "krylov_total", "back_total"):
+        assert r1[k] == r2[k], k
+    assert r1["current_t"] == t2 and r1["delt"] == d2
+    assert np.array_equal(o1.get_state()["head_new"], h2)
