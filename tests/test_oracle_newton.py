@@ -4,7 +4,9 @@ written out again in Python from the Fortran and driven by the oracle's own make
 solve_linalg, calc_func and calc_vecjacf (each pinned separately in test_oracle_kat.py):
 the oracle's Newton solve must land on the same heads, bit for bit, with the same Newton,
 Krylov and backtracking counts.  This pins the Newton controller -- the inexact-Newton
-forcing, the step-length cap and the cubic/quadratic line search -- against the source.
+forcing, the step-length cap and the cubic/quadratic line search -- against the source,
+including quirk Q2 of the reference AMG mode (the slope reads the preconditioner's last
+input, which loop_amg leaves in rhs, Linear_solution.f90:516-529,717-718).
 The time loop around it (accept, reject and roll back, dt control, the real(SP) clock) is
 restated the same way.
 """
@@ -47,6 +49,40 @@ def _abserrmax(x_new, x_pre):
         if abs(a) >= aval:
             aval, bval = abs(a), a
     return bch, bval, nun
+
+
+def _bicgs(o, b, bnorm, errtol, maxit):
+    """solve_bicgs from x = 0 (Linear_solution.f90:234-493) with the oracle's matvec and
+    preconditioner; returns x, ||r||^2, iterations, convergence flag and the last vector
+    handed to the preconditioner (which loop_amg leaves in rhs, quirk Q2)."""
+    x, resi, p, v = np.zeros_like(b), b.copy(), np.zeros_like(b), np.zeros_like(b)
+    rs = resi.copy()
+    sk0, alpha, omega, rnorm, last = np.inf, 0.0, 1.0, 0.0, None
+    for it in range(1, maxit + 1):
+        sk = _dot(resi, rs)
+        p = resi.copy() if it == 1 else resi + ((sk / sk0) * (alpha / omega)) * (p - omega * v)
+        last = p
+        z = o.precond(p)
+        v = o.matvec(z)
+        alpha = sk / _dot(v, rs)
+        x = x + alpha * z
+        resi = resi - alpha * v
+        rnorm = _dot(resi, resi)
+        if math.sqrt(rnorm / bnorm) <= errtol:
+            return x, rnorm, it, 1, last
+        last = resi
+        z = o.precond(resi)
+        t = o.matvec(z)
+        omega = _dot(t, resi) / _dot(t, t)
+        x = x + omega * z
+        resi = resi - omega * t
+        rnorm = _dot(resi, resi)
+        if math.sqrt(rnorm / bnorm) <= errtol:
+            return x, rnorm, it, 1, last
+        if it == maxit:
+            return x, rnorm, it, 0, last
+        sk0 = sk
+    raise AssertionError("unreachable")
 
 
 class _Newton:
@@ -161,7 +197,11 @@ class _Newton:
                 l2_pre, eta = l2_new, 0.5
             h_pre = h
             errtol = prm["lin_tol"] if prm["lin_tol"] > 0 else eta
-            dh, l2_jnorm, it, conv = o.solve_linalg(l2_pre, errtol)
+            if prm["precon_type"] == 1 and prm["ref_quirks"]:
+                # Q2: loop_amg leaves its last input in rhs, which the line-search slope reads
+                dh, l2_jnorm, it, conv, rhs = _bicgs(o, rhs, l2_pre, errtol, prm["maxinn_iter"])
+            else:
+                dh, l2_jnorm, it, conv = o.solve_linalg(l2_pre, errtol)
             inner += it
             h = h_pre + dh
             maxvar, maxunk, _ = _abserrmax(h, h_pre)
@@ -205,7 +245,9 @@ class _Newton:
 
 
 def _case(name, kw, amp, seed):
-    p = make_config(name, precon_type=0, **kw)
+    kw = dict(kw)
+    kw.setdefault("precon_type", 0)
+    p = make_config(name, **kw)
     h0 = p.head0 + amp * np.random.default_rng(seed).standard_normal(p.ncalc) / p.params["len_scal"]
     pair = []
     for _ in range(2):
@@ -221,12 +263,14 @@ def _case(name, kw, amp, seed):
     ("hetero", dict(shape=(10, 8, 6), seed=3, maxinn_iter=3), 0.3, 1),   # inexact solves, rough start
     ("hetero", dict(shape=(10, 8, 6), seed=3, maxinn_iter=2), 1.0, 2),   # 18 backtracks, Newton cap
     ("hetero", dict(shape=(10, 8, 6), seed=7, maxinn_iter=1), 2.0, 4),   # 24 backtracks, Newton cap
+    ("hetero", dict(shape=(10, 8, 6), seed=3, precon_type=1, ref_quirks=1), 0.0, 0),   # quirks Q1, Q2
+    ("hetero", dict(shape=(10, 8, 6), seed=3, precon_type=1, ref_quirks=1, maxinn_iter=3), 0.3, 1),
 ])
 def test_newton_controller_restated(name, kw, amp, seed):
     p, (o1, o2) = _case(name, kw, amp, seed)
     rc, st = o1.calc_numsol()
     h1 = o1.get_state()["head_new"]
-    h2, status, out_iter, inner, backs, maxvar, l2 = _Newton(o2, dict(p.params, precon_type=0, **kw)).solve(
+    h2, status, out_iter, inner, backs, maxvar, l2 = _Newton(o2, p.params).solve(
         o2.get_state()["head_new"].copy())
     assert (rc, st["out_iter"], st["inner_total"], st["back_total"]) == (status, out_iter, inner, backs)
     assert np.array_equal(h1, h2)
