@@ -3,8 +3,8 @@
 Times the candidate block sizes of the kernels whose launch shape is free (the van
 Genuchten/storage pass and the level-1 V-cycle smoother; kernels with reductions keep a
 fixed shape so results never depend on the tuning) with msg_gpu_kernel_time on the
-solver's own state, and caches the choice per (nx, ny, nz, precision) in a JSON file
-($MSG123_TUNE_CACHE, default ~/.cache/msg123_b200/tuning.json).
+solver's own state, and caches the choice per (nx, ny, nz, precision, kr form) in a JSON
+file ($MSG123_TUNE_CACHE, default ~/.cache/msg123_b200/tuning.json).
 """
 import json
 import os
@@ -37,7 +37,7 @@ def _save(d):
 
 def key(solver):
     p = solver.prob
-    return f"{p.nx}x{p.ny}x{p.nz}:p{solver.params['precision']}"
+    return f"{p.nx}x{p.ny}x{p.nz}:p{solver.params['precision']}:v{solver.params.get('vg_form', 0)}"
 
 
 def tune(solver, reps=5, use_cache=True):
