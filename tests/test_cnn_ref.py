@@ -1,5 +1,6 @@
-"""Pins the numpy reference of the learned-guess network: its analytic gradients must
-match central finite differences in float64 (no GPU needed)."""
+"""Pins the numpy reference of the learned-guess network (no GPU needed): its analytic
+gradients match central finite differences in float64, its convolution matches the
+definition written out as loops, and its bfloat16 rounding matches torch's."""
 import numpy as np
 
 from oracle import cnn_ref
@@ -49,3 +50,38 @@ def test_reference_gradients_match_finite_differences():
         ls[l][1][0] -= 2 * eps
         dn = loss_of(ls)
         assert abs((up - dn) / (2 * eps) - grads[l][1][0]) <= 1e-6 * max(1e-3, abs(grads[l][1][0]))
+
+
+def test_conv_matches_a_direct_loop():
+    """The reference convolution against the definition written out as loops: tap t is
+    (dz, dy, dx) = (t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1), W[t][co][ci], zero padding."""
+    rng = np.random.default_rng(4)
+    nz, ny, nx = 3, 4, 5
+    x = rng.standard_normal((nz, ny, nx, 16))
+    W = rng.standard_normal((27, 16, 16))
+    b = rng.standard_normal(16)
+    out = cnn_ref.conv(x, W, b)
+    ref = np.zeros_like(out)
+    for z in range(nz):
+        for y in range(ny):
+            for xx in range(nx):
+                acc = b.copy()
+                for t in range(27):
+                    dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+                    zz, yy, xs = z + dz, y + dy, xx + dx
+                    if 0 <= zz < nz and 0 <= yy < ny and 0 <= xs < nx:
+                        acc += W[t] @ x[zz, yy, xs]
+                ref[z, y, xx] = acc
+    assert np.max(np.abs(out - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_bf16_rounding_is_nearest_even():
+    """cnn_ref.bf16 against torch's float32 -> bfloat16 conversion (round to nearest, ties
+    to even), including exact ties and values near the overflow of the exponent."""
+    import torch
+    rng = np.random.default_rng(5)
+    a = np.concatenate([rng.standard_normal(10000).astype(np.float32),
+                        np.array([1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -1.0 - 2.0 ** -8, 0.0, -0.0,
+                                  3.3895e38, 1e-40], dtype=np.float32)])
+    want = torch.from_numpy(a).to(torch.bfloat16).to(torch.float64).numpy()
+    assert np.array_equal(cnn_ref.bf16(a), want)
