@@ -43,3 +43,17 @@ def test_no_sweeps():
     restrict = 4 * 100 + 8 * 1500 + 4 * 1000 + 4 * 100
     prolong = 4 * 1000 + 8 * 1500 + 4 * 100 + 8 * 1000
     assert got == pytest.approx(fine + res + restrict + prolong + 8 * 100 * 100 + 8 * 100)
+
+
+def test_clock_summary_from_samples():
+    """The clocks key of the bench line: median SM clock, highest max clock and every
+    throttle reason seen Active in any sample (nvidia-smi csv, noheader, nounits)."""
+    cs = bench.ClockSampler()
+    assert cs.summary()["reasons"] == ["unsampled"]
+    cs.samples = [["1965", "1965", "700.1", "Not Active", "Not Active", "Not Active", "Not Active"],
+                  ["1950", "1965", "980.0", "Not Active", "Not Active", "Not Active", "Active"],
+                  ["1980", "1965", "990.5", "Not Active", "Not Active", "Not Active", "Active"],
+                  ["[N/A]", "1965", "[N/A]", "Not Active", "Active", "Not Active", "Not Active"]]
+    s = cs.summary()
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 4
+    assert s["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
