@@ -41,7 +41,7 @@ METRIC = "cell-timesteps/s at 1e-8 rel head tol"
 # by its 4,194,304 cells; traffic grows in proportion to the cells.
 TRAFFIC_CALC_FUNC_PER_CELL = 150.0
 TRAFFIC_SOURCE = "profiles/calc_func_kernels_hetero_256x256x64.md, scaled by cells"
-PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 # Algorithmic bytes per cell of the kernels timed by msg_gpu_kernel_time (compulsory
 # HBM traffic, neighbour reads cache-reused):
@@ -101,12 +101,25 @@ def vcycle_bytes(sizes, sweeps, coarse_max):
 CNN_FLOP_PER_CELL = 4 * 27 * 16 * 16 * 2
 
 
-def load_peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
+def _peak_value(v):
+    """A peak given as a number, or as a record holding it under "value"."""
+    if isinstance(v, dict):
+        v = v.get("value")
+    return float(v)
+
+
+def load_peaks(path=None):
+    """(HBM GB/s, bf16 TFLOP/s, source) from MEASURED_PEAKS.json, else the fallback figures
+    measured earlier on this hardware; an unreadable file falls back too and says so."""
+    p = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if not os.path.exists(p):
+        return PEAKS_FALLBACK["hbm_gbs"], PEAKS_FALLBACK["bf16_tflops"], "fallback"
+    try:
         with open(p) as f:
-            return json.load(f), "measured"
-    return PEAKS_FALLBACK, "fallback"
+            d = json.load(f)
+        return _peak_value(d["hbm_gbs"]), _peak_value(d.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"])), "measured"
+    except (OSError, ValueError, TypeError, KeyError):
+        return PEAKS_FALLBACK["hbm_gbs"], PEAKS_FALLBACK["bf16_tflops"], "fallback (measured peaks file unreadable)"
 
 
 class ClockSampler:
@@ -314,9 +327,7 @@ def main():
     value = reduce(dist, float(prob.ncalc * st["accepted"]), "sum") / (tmax * 1e-3)
 
     # kernel timings for the roofline (state of the last timed step, library stream)
-    peaks, src = load_peaks()
-    hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
-    tc_peak = float(peaks.get("bf16_tflops", 1590.0))
+    hbm, tc_peak, src = load_peaks()
     # the V-cycle first: make_matvec below re-assembles at the converged head, whose
     # right-hand side is far smaller than any the solve passes to the preconditioner
     t_prec = g.kernel_time(3, reps=5)

@@ -57,3 +57,16 @@ def test_clock_summary_from_samples():
     s = cs.summary()
     assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 4
     assert s["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+
+
+def test_load_peaks(tmp_path):
+    import json
+    assert bench.load_peaks(str(tmp_path / "absent.json"))[2] == "fallback"
+    p = tmp_path / "peaks.json"
+    p.write_text(json.dumps({"hbm_gbs": 6543.7, "bf16_tflops": 1642.7, "bf16_tflops_sustained": 1400.0}))
+    assert bench.load_peaks(str(p)) == (6543.7, 1642.7, "measured")
+    p.write_text(json.dumps({"hbm_gbs": {"value": 6500.0}, "bf16_tflops": {"value": 1600.0}}))
+    assert bench.load_peaks(str(p)) == (6500.0, 1600.0, "measured")
+    p.write_text("{not json")
+    hbm, tc, src = bench.load_peaks(str(p))
+    assert (hbm, tc) == (6650.0, 1590.0) and src.startswith("fallback")
