@@ -174,6 +174,18 @@ def make_box(shape=(20, 20, 50), d=(0.1, 0.1, 0.1), nsteps=48, **pkw):
                    sea, head0, np.zeros(nx * ny), 1.0e30, 1.0, nsteps, prm)
 
 
+def make_box1r(shape=(20, 20, 50), nsteps=48, criteria=1.0e-6, **pkw):
+    """The box in a form the reference itself can run ("config 1R"): the same ponded sea
+    layer on top, but a no-flow bottom (no free drainage), the Eisenstat-Walker linear
+    tolerance (lin_tol = 0) and an absolute Newton criterion in metres (criteria_rel = 0),
+    i.e. only features the reference's input decks can express."""
+    import dataclasses
+    p = make_box(shape=shape, nsteps=nsteps)
+    prm = dict(p.params, lin_tol=0.0, criteria_rel=0, criteria=criteria)
+    prm.update(pkw)
+    return dataclasses.replace(p, name="box1r", free_drainage=0, params=prm)
+
+
 def make_hetero(shape=(256, 256, 64), d=(1.0, 1.0, 0.25), seed=2024, sigma=1.0, corr=(20, 20, 4),
                 nsteps=96, wt_depth=None, rain_mm_h=20.0, rain_hours=6.0, **pkw):
     """Heterogeneous block: lnKs GRF, random van Genuchten draws, hydrostatic start."""
@@ -229,6 +241,8 @@ def make_member(seed, **pkw):
 def make_config(name, **kw):
     if name == "box":
         return make_box(**kw)
+    if name == "box1r":
+        return make_box1r(**kw)
     if name == "hetero":
         return make_hetero(**kw)
     if name == "large":

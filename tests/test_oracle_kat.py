@@ -764,3 +764,18 @@ def test_calc_mass_restated(name, kw):
             dh = float(p.sea_head[s]) - float(h[s])
             acc[7] += float(p.ksz[s]) * kr[s] * (far[0, s] / dis[0, s]) * dh * delt
     assert np.array_equal(got, np.array(acc))
+
+
+def test_reference_expressible_box():
+    """Config 1R (sea-layer top, no-flow bottom, Eisenstat-Walker tolerance, absolute
+    criterion): water ponded on the top enters through the sea faces and is all stored --
+    no drainage volume, and the step's volumes balance."""
+    p = make_config("box1r", shape=(6, 5, 10), nsteps=3)
+    assert p.free_drainage == 0 and p.params["lin_tol"] == 0.0 and p.params["criteria_rel"] == 0
+    o = Oracle(p)
+    o.init_state()
+    rc, st = o.advance(nsteps=3)
+    assert rc == 0 and st["accepted"] == 3
+    m = o.calc_mass()
+    assert m[8] == 0.0 and m[7] > 0.0          # no drainage; inflow from the ponded layer
+    assert abs(m[0] + m[1] + m[4] + m[7]) <= 1e-10 * m[7]       # measured 2.7e-12
