@@ -331,11 +331,12 @@ def _seq_dot(a, b):
     return s
 
 
-def _bicgs(o, b, bnorm, errtol, maxit):
-    """solve_bicgs (Linear_solution.f90:234-493) written out again from the Fortran, from
-    inx = 0 (so resi = b), with the oracle's own matvec and DILU apply and sequential sums."""
-    x = np.zeros_like(b)
-    resi = b.copy()
+def _bicgs(o, b, bnorm, errtol, maxit, x0=None):
+    """solve_bicgs (Linear_solution.f90:234-493) written out again from the Fortran, with the
+    oracle's own matvec and DILU apply and sequential sums; the first residual is calc_resi
+    (Calc_simulation.f90:36-73: b - (d x + the row's entries in order)), i.e. b - A x0."""
+    x = np.zeros_like(b) if x0 is None else x0.copy()
+    resi = b.copy() if x0 is None else b - o.matvec(x0)
     rs = resi.copy()
     p = np.zeros_like(b)
     v = np.zeros_like(b)
@@ -367,8 +368,8 @@ def _bicgs(o, b, bnorm, errtol, maxit):
     return x, rnorm, maxit
 
 
-@pytest.mark.parametrize("maxit", [1, 2, 4])
-def test_bicgstab_recurrence_restated_twice(maxit):
+@pytest.mark.parametrize("maxit,start", [(1, False), (2, False), (4, False), (3, True)])
+def test_bicgstab_recurrence_restated_twice(maxit, start):
     """The oracle's BiCGStab against a second restatement of the same Fortran: identical
     iterates, residual norm and iteration count, bit for bit."""
     p = make_config("hetero", shape=(10, 8, 6), seed=5, precon_type=0, maxinn_iter=maxit)
@@ -378,8 +379,9 @@ def test_bicgstab_recurrence_restated_twice(maxit):
     d, lu, b = o.make_matvec()
     o.set_system(d, lu, b)
     bnorm = _seq_dot(b, b)
-    xo, last, it, _ = o.solve_linalg(bnorm, 1e-30)
-    xp, rn, itp = _bicgs(o, b, bnorm, 1e-30, maxit)
+    x0 = 0.1 * np.random.default_rng(2).standard_normal(p.ncalc) if start else None
+    xo, last, it, _ = o.solve_linalg(bnorm, 1e-30, x0=x0)
+    xp, rn, itp = _bicgs(o, b, bnorm, 1e-30, maxit, x0=x0)
     assert it == itp == maxit
     assert np.array_equal(xo, xp) and last == rn
 
