@@ -70,3 +70,57 @@ def test_load_peaks(tmp_path):
     p.write_text("{not json")
     hbm, tc, src = bench.load_peaks(str(p))
     assert (hbm, tc) == (6650.0, 1590.0) and src.startswith("fallback")
+
+
+class _FakeSolver:
+    """Stands in for GpuSolver in a dry run of bench.main: fixed kernel times, one AMG level
+    pair, a state of the right size."""
+
+    def __init__(self, prob, **kw):
+        self.prob, self.params = prob, dict(prob.params, **kw)
+
+    def init_state(self):
+        pass
+
+    def advance(self, nsteps=1, **kw):
+        return 0, dict(accepted=nsteps, rejected=0, newton_total=5 * nsteps, krylov_total=5 * nsteps,
+                       back_total=0, current_t=600.0 * nsteps, delt=600.0, status=0)
+
+    def timers(self):
+        return {"total_ms": 10.0}
+
+    def kernel_time(self, which, reps=1):
+        return {0: 0.01, 1: 0.02, 2: 0.03, 3: 0.05, 4: 1.0, 5: 0.2}[which]
+
+    def amg_sizes(self):
+        n = self.prob.ncalc
+        return [(n, 6 * n, 0), (n // 8, n, n)]
+
+    def close(self):
+        pass
+
+
+def test_bench_main_dry_run(monkeypatch, capsys):
+    """bench.main on the CPU with stand-ins for the CUDA solver and the network: the JSON
+    line carries every key of the contract, with values derived from the stand-ins."""
+    import json
+    import sys
+    from msg123_b200 import learned, solver, train_guess
+    monkeypatch.setattr(solver, "GpuSolver", _FakeSolver)
+    monkeypatch.setattr(solver, "launch_count", lambda: 0)
+    monkeypatch.setattr(learned, "Cnn", lambda seed=0: type("C", (), {"attach": lambda s, g: None,
+                                                                       "close": lambda s: None})())
+    monkeypatch.setattr(train_guess, "load", lambda c: c)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "hetero", "--shape", "8x8x4", "--steps", "2",
+                                      "--warmup", "3", "--no-cpu", "--no-e2e", "--no-plain"])
+    bench.main()
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "roofline", "cpu_baseline", "e2e",
+              "gpu_launches", "clocks"):
+        assert k in line, k
+    assert line["value"] == pytest.approx(256 * 2 / 10e-3)
+    r = line["roofline"]
+    assert r["ms_per_launch"] == 0.02 and r["unit"] == "GB/s" and 0 < r["frac"]
+    assert r["others"]["mixed V-cycle, all levels"]["ms"] == 0.05
+    assert r["vcycle_mixed_ms"] == 0.05 and line["config"]["workload"].startswith("hetero 8x8x4")
