@@ -100,7 +100,8 @@ class _FakeSolver:
         pass
 
 
-def test_bench_main_dry_run(monkeypatch, capsys):
+@pytest.mark.parametrize("extra", [["--no-cpu", "--no-plain"], ["--cpu-shape", "8x8x4", "--plain-steps", "2"]])
+def test_bench_main_dry_run(monkeypatch, capsys, extra):
     """bench.main on the CPU with stand-ins for the CUDA solver and the network: the JSON
     line carries every key of the contract, with values derived from the stand-ins."""
     import json
@@ -112,7 +113,7 @@ def test_bench_main_dry_run(monkeypatch, capsys):
                                                                        "close": lambda s: None})())
     monkeypatch.setattr(train_guess, "load", lambda c: c)
     monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "hetero", "--shape", "8x8x4", "--steps", "2",
-                                      "--warmup", "3", "--no-cpu", "--no-e2e", "--no-plain"])
+                                      "--warmup", "3", "--no-e2e"] + extra)
     bench.main()
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
@@ -124,3 +125,7 @@ def test_bench_main_dry_run(monkeypatch, capsys):
     assert r["ms_per_launch"] == 0.02 and r["unit"] == "GB/s" and 0 < r["frac"]
     assert r["others"]["mixed V-cycle, all levels"]["ms"] == 0.05
     assert r["vcycle_mixed_ms"] == 0.05 and line["config"]["workload"].startswith("hetero 8x8x4")
+    if "--no-cpu" not in extra:                       # the oracle really ran on the 8x8x4 sample
+        cb = line["cpu_baseline"]
+        assert cb["kind"] == "port" and cb["value"] > 0 and "8x8x4" in cb["sample"]
+        assert line["plain_fp64"]["ms_per_step"] == pytest.approx(5.0)
