@@ -96,11 +96,19 @@ class _FakeSolver:
         n = self.prob.ncalc
         return [(n, 6 * n, 0), (n // 8, n, n)]
 
+    def get_state(self, out=None):
+        return out
+
+    def set_state(self, **kw):
+        pass
+
     def close(self):
         pass
 
 
-@pytest.mark.parametrize("extra", [["--no-cpu", "--no-plain"], ["--cpu-shape", "8x8x4", "--plain-steps", "2"]])
+@pytest.mark.parametrize("extra", [["--no-cpu", "--no-plain", "--no-e2e"],
+                                   ["--cpu-shape", "8x8x4", "--plain-steps", "2", "--no-e2e"],
+                                   ["--no-cpu", "--no-plain"]])
 def test_bench_main_dry_run(monkeypatch, capsys, extra):
     """bench.main on the CPU with stand-ins for the CUDA solver and the network: the JSON
     line carries every key of the contract, with values derived from the stand-ins."""
@@ -112,8 +120,11 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
     monkeypatch.setattr(learned, "Cnn", lambda seed=0: type("C", (), {"attach": lambda s, g: None,
                                                                        "close": lambda s: None})())
     monkeypatch.setattr(train_guess, "load", lambda c: c)
+    import torch
+    empty = torch.empty
+    monkeypatch.setattr(torch, "empty", lambda *a, pin_memory=False, **k: empty(*a, **k))   # no CUDA here
     monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "hetero", "--shape", "8x8x4", "--steps", "2",
-                                      "--warmup", "3", "--no-e2e"] + extra)
+                                      "--warmup", "3"] + extra)
     bench.main()
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
@@ -125,6 +136,10 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
     assert r["ms_per_launch"] == 0.02 and r["unit"] == "GB/s" and 0 < r["frac"]
     assert r["others"]["mixed V-cycle, all levels"]["ms"] == 0.05
     assert r["vcycle_mixed_ms"] == 0.05 and line["config"]["workload"].startswith("hetero 8x8x4")
+    if "--no-e2e" not in extra:                       # pinned host state in and out every step
+        e = line["e2e"]
+        assert e["h2d_bytes_per_step"] == 3 * 256 * 8 + 64 * 8 and e["d2h_bytes_per_step"] == 4 * 256 * 8 + 64 * 8
+        assert e["value"] > 0
     if "--no-cpu" not in extra:                       # the oracle really ran on the 8x8x4 sample
         cb = line["cpu_baseline"]
         assert cb["kind"] == "port" and cb["value"] > 0 and "8x8x4" in cb["sample"]
