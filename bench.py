@@ -178,10 +178,12 @@ def dist_setup():
     import torch.distributed as dist
     rank = int(os.environ["RANK"])
     local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
+    backend = "nccl" if torch.cuda.is_available() else "gloo"   # gloo: the CPU tests of this path
+    if backend == "nccl":
+        torch.cuda.set_device(local)
     # short enough that ranks left waiting for a failed one end with an error soon; the
     # longest gap between two collectives (field generation, context build) is seconds
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
     return rank, ws, dist
 
 

@@ -1,5 +1,7 @@
-"""The algorithmic-byte model behind the V-cycle roofline entry of bench.py, counted by
-hand on small hierarchies (no GPU)."""
+"""bench.py without a GPU: the algorithmic-byte model behind the V-cycle roofline entry
+(counted by hand on small hierarchies), the clocks summary, the measured-peaks reader, and
+dry runs of the whole benchmark -- one rank, and two ranks over gloo -- with stand-ins for
+the CUDA solver, so every key of the JSON line and the multi-rank reductions are checked."""
 import importlib.util
 import os
 
@@ -144,3 +146,48 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
         cb = line["cpu_baseline"]
         assert cb["kind"] == "port" and cb["value"] > 0 and "8x8x4" in cb["sample"]
         assert line["plain_fp64"]["ms_per_step"] == pytest.approx(5.0)
+
+
+def _bench_rank(rank, world, port, q):
+    """One rank of a two-rank bench run over gloo, with the stand-ins of the dry run."""
+    import contextlib
+    import io
+    import sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), LOCAL_RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    from msg123_b200 import learned, solver, train_guess
+    solver.GpuSolver = _FakeSolver
+    solver.launch_count = lambda: 0
+    learned.Cnn = lambda seed=0: type("C", (), {"attach": lambda s, g: None, "close": lambda s: None})()
+    train_guess.load = lambda c: c
+    sys.argv = ["bench.py", "--workload", "hetero", "--shape", "8x8x4", "--steps", "2", "--warmup", "3",
+                "--gpus", str(world), "--no-cpu", "--no-plain", "--no-e2e"]
+    out = io.StringIO()
+    with contextlib.redirect_stdout(out):
+        bench.main()
+    q.put((rank, out.getvalue()))
+
+
+def test_bench_two_ranks_over_gloo():
+    """bench.py under two ranks (gloo on CPU): only rank 0 prints, and the value is the
+    cells x steps of both ranks over the slowest rank's time."""
+    import json
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_bench_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    outs = dict(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert outs[1].strip() == ""
+    line = json.loads(outs[0].strip().splitlines()[-1])
+    assert line["n_gpus"] == 2 and line["value"] == pytest.approx(2 * 256 * 2 / 10e-3)
+    assert line["config"]["parallelism"] == "replicas x2"
