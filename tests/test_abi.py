@@ -110,3 +110,15 @@ def test_missing_library_fails_loudly(monkeypatch):
     monkeypatch.setattr(solver, "LIB_PATH", "/nonexistent/libmsg123gpu.so")
     with pytest.raises(solver.MsgError, match="missing"):
         solver.load_library()
+
+
+def test_smoke_fails_loudly_without_a_gpu():
+    """On a machine without a GPU the smoke check raises the library's CUDA error instead of
+    passing on some host path."""
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    import __graft_entry__ as entry
+    from msg123_b200.solver import MsgError
+    with pytest.raises(MsgError, match="err_cuda"):
+        entry.smoke()
