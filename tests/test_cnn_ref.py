@@ -85,3 +85,19 @@ def test_bf16_rounding_is_nearest_even():
                                   3.3895e38, 1e-40], dtype=np.float32)])
     want = torch.from_numpy(a).to(torch.bfloat16).to(torch.float64).numpy()
     assert np.array_equal(cnn_ref.bf16(a), want)
+
+
+def test_shipped_weights_are_well_formed():
+    """The committed network (msg123_b200/weights/guess_cnn.npy): one float32 vector of the
+    four layers' taps and biases, finite, and the float64 reference runs it on a small
+    grid to a finite output."""
+    import os
+    from msg123_b200.learned import unpack
+    w = np.load(os.path.join(os.path.dirname(__file__), "..", "msg123_b200", "weights", "guess_cnn.npy"))
+    assert w.dtype == np.float32 and w.shape == (4 * (27 * 16 * 16 + 16),)
+    assert np.all(np.isfinite(w))
+    layers = [(cnn_ref.bf16(W), b.astype(np.float64)) for W, b in unpack(w)]
+    x = np.zeros((3, 4, 5, 16))
+    x[..., :7] = cnn_ref.bf16(np.random.default_rng(6).standard_normal((3, 4, 5, 7)))
+    _, out, _ = cnn_ref.loss_and_grad(layers, x, np.zeros((3, 4, 5)))
+    assert np.all(np.isfinite(out))
