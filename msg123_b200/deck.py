@@ -69,13 +69,34 @@ def _value(tok):
         return float(t.replace("d", "e"))
 
 
+def _groups(text):
+    """(name, body) of each &name ... / group; a '/' or '&end' inside quotes does not close it."""
+    i, n = 0, len(text)
+    while True:
+        m = re.compile(r"&(\w+)", re.I).search(text, i)
+        if not m:
+            return
+        j, q = m.end(), None
+        while j < n:
+            ch = text[j]
+            if q:
+                if ch == q:
+                    q = None
+            elif ch in "'\"":
+                q = ch
+            elif ch == "/" or text[j:j + 4].lower() == "&end":
+                break
+            j += 1
+        yield m.group(1).lower(), text[m.end():j]
+        i = j + 1
+
+
 def read_namelists(text):
     """{group: {name: value or list of values}} from Fortran namelist text (groups opened by
     &name and closed by / or &end; names case-insensitive; r*v repeat counts; ! comments)."""
     text = "\n".join(_strip_comment(l) for l in text.splitlines())
     groups = {}
-    for m in re.finditer(r"&(\w+)(.*?)(?:/|&end\b)", text, re.S | re.I):
-        name, body = m.group(1).lower(), m.group(2)
+    for name, body in _groups(text):
         toks = [t for t in _tokens(body) if t != ","]
         vals, key, cur = {}, None, []
         i = 0

@@ -31,6 +31,11 @@ def test_namelist_parser():
     assert g["set_calc_time"]["calc_unit"] == "HOU"
     assert g["set_solution"]["criteria"] == 1.0e-4 and g["set_solution"]["maxinn_iter"] == 50
     assert g["misc"] == {"flags": [True, True, True, False], "name": "it's"}
+    # a '/' or '!' inside quotes neither closes the group nor starts a comment; &end closes too
+    h = deck.read_namelists("&set_grid grid_file = 'in/grid!1.txt', gridx = 2 /\n"
+                            "&set_calc_time sdate = 6*0, end_time = 3.6d3 &end\n&set_simulation sim_type=0/")
+    assert h["set_grid"] == {"grid_file": "in/grid!1.txt", "gridx": 2}
+    assert h["set_calc_time"] == {"sdate": [0] * 6, "end_time": 3600.0} and h["set_simulation"] == {"sim_type": 0}
 
 
 def test_solver_params_from_a_transient_deck():
