@@ -8,9 +8,12 @@
  * Parity status: the reference is Fortran 2008 and no Fortran compiler exists
  * on the build or GPU machines, and the reference ships no tests, fixtures or
  * golden vectors.  Parity is therefore UNPINNED by the reference itself; the
- * restatement is pinned by analytic known-answer tests instead (van Genuchten
- * closed forms, hydrostatic equilibrium F == 0, finite-difference Jacobian
- * against the analytic derivative, mass closure) in tests/test_oracle_kat.py.
+ * restatement is pinned instead by analytic known-answer tests (van Genuchten
+ * closed forms, exact steady states, harmonic conductances, mass closure, the dt
+ * heuristic, quirk Q1) and by second restatements written in Python from the
+ * Fortran that it matches bit for bit (residual, Jacobian, Krylov, AMG
+ * prolongation, Newton controller, time loop): tests/test_oracle_kat.py and
+ * tests/test_oracle_newton.py.
  *
  * Every routine cites the reference file:line it restates (paths relative to
  * the Msg123 source tree).  Evaluation order of products and sums follows the
