@@ -160,8 +160,12 @@ MSG_API int msg_gpu_get_connect(msg_ctx_t *ctx, int32_t *offind, int32_t *offrow
                         int32_t *left_off, int32_t *right_off, double *hydf_conn,
                         double *abyd_conn, int32_t *nnz);
 
-/* Set the time-level state (head_new, head_old, srat_old, surf_head, surf_old)
- * and delt.  NULL leaves a field unchanged. */
+/* Set the time-level state and delt.  NULL (or delt <= 0) leaves a field unchanged.
+ * surf_head sets BOTH the surface head and surf_old, the surface head a rejected step
+ * rolls back to (Time_module.f90:253-264): a host that passes surf_head in the middle
+ * of a step therefore also moves that rollback point.  A host that restores a saved
+ * state between steps passes the surf_head it read with msg_gpu_get_state, which is
+ * then the rollback point of the next step as in the reference. */
 MSG_API int msg_gpu_set_state(msg_ctx_t *ctx, const double *head_new, const double *head_old,
                       const double *srat_old, const double *surf_head, double delt);
 MSG_API int msg_gpu_get_state(msg_ctx_t *ctx, double *head_new, double *head_old, double *srat_new,
@@ -217,6 +221,16 @@ MSG_API int msg_gpu_advance(msg_ctx_t *ctx, int32_t nsteps, double rech_until, d
  * storage, flow, recharge, well, surface, river, lake, sea (+ out[8] drainage),
  * each a volume over the step (rate * delt). */
 MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
+/* calc_cell_mas (Calc_output.f90:54-91, through calc_mass with sfla = 0): the step's
+ * volumes per cell, in the arrays the reference adds into st_msloc for every regional
+ * mass-balance output.  sto, con, sea, wel: [ncalc] (storage change, flow from the
+ * neighbours, sea-face inflow, wells); rec, sur, riv, lak: [ncals] (recharge, surface,
+ * river, lake); drn: [ncals] outflow through the bottom face of each column under free
+ * drainage (extension, no reference column).  Each a rate times delt, summing to the
+ * msg_gpu_calc_mass totals.  No wells, rivers or lakes are modelled, so wel, riv and lak
+ * come back zero.  Any pointer may be NULL. */
+MSG_API int msg_gpu_cell_mass(msg_ctx_t *ctx, double *sto, double *con, double *sea, double *wel, double *rec,
+                              double *sur, double *riv, double *lak, double *drn);
 /* Water table of the current state (calc_wtable, Calc_output.f90:20-52, called by
  * write_out_wtabf with head_new and srat_new): for each surface column, the head of the
  * lowest cell that is not fully saturated (srat != 1), scanning up from the bottom layer;
@@ -269,9 +283,12 @@ MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv);
  * under a fixed device-memory budget).  No counterpart exists in the reference.
  * a_dev / inv_dev: caller-owned device arrays, row-major n x n, 1 <= n <= 512 (larger n
  * returns MSG_ERR_SIZE).  Work is queued on `stream` (NULL: legacy default stream).
- * The workspace is one static device array per GPU (about 4 MiB, held until exit);
- * the first call on a device looks up its address and should precede any stream
- * capture; concurrent calls on one device race on that workspace. */
+ * The workspace is one static device array per GPU (about 4 MiB, held until exit).
+ * Every call looks up its address for the current device (so a cudaDeviceReset between
+ * calls is safe); the first call on a device also loads the library's device code there
+ * and should precede any stream capture.  Concurrent calls on one device race on that
+ * workspace.  A singular input is not detected: its zero pivot gives inf/NaN entries
+ * and the call still returns MSG_OK. */
 MSG_API int msg_gpu_dense_inverse_noalloc(int32_t n, const double *a_dev, double *inv_dev, void *stream);
 
 /* ---- learned Newton initial guess (no counterpart in the reference) ----------------------

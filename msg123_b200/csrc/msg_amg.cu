@@ -18,7 +18,6 @@
 #include <cuda_bf16.h>
 #include <vector>
 #include <algorithm>
-#include <mutex>
 
 namespace cg = cooperative_groups;
 
@@ -1439,26 +1438,21 @@ int amg_apply(msg_ctx *c, const double *r, double *z) {
 constexpr int kNoAllocMaxN = 512;
 static __device__ __align__(256) double g_noalloc_gj[(size_t)2 * kNoAllocMaxN * kNoAllocMaxN + 32];
 
-static double *g_noalloc_addr[64];   // device address of g_noalloc_gj, per device (host side)
-static std::mutex g_noalloc_mu;
-
 // In host code g_noalloc_gj names a host-side stand-in, not device memory: the device
-// address must come from cudaGetSymbolAddress, once per device, with that device current.
+// address comes from cudaGetSymbolAddress with the caller's device current.  It is looked
+// up again on every call rather than cached: after a cudaDeviceReset the runtime builds a
+// new primary context and reloads this module, and the array may then sit elsewhere, so
+// an address kept from before the reset would point into freed memory.  The lookup is a
+// host-side table search (the module is loaded by the first call), far cheaper than the
+// three kernels it precedes.
 static int noalloc_scratch(double **out) {
-  int dev = 0;
-  MSG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) { ::msg::set_error("dense_inverse_noalloc: device %d out of range", dev); return MSG_ERR_ARG; }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_gj);
-    if (e != cudaSuccess || !p) {
-      ::msg::set_error("dense_inverse_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-      return MSG_ERR_CUDA;
-    }
-    g_noalloc_addr[dev] = static_cast<double *>(p);
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_gj);
+  if (e != cudaSuccess || !p) {
+    ::msg::set_error("dense_inverse_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    return MSG_ERR_CUDA;
   }
-  *out = g_noalloc_addr[dev];
+  *out = static_cast<double *>(p);
   return MSG_OK;
 }
 
@@ -1503,10 +1497,13 @@ MSG_API int msg_gpu_dense_inverse(int32_t n, const double *a, double *inv) {
 // Same result as msg_gpu_dense_inverse, bit for bit, without any allocation: a_dev and
 // inv_dev are device arrays (row-major n x n) owned by the caller; the work runs on
 // `stream` (NULL: the legacy default stream) and is complete when that stream is.
-// The first call on a device looks up the scratch address (cudaGetSymbolAddress); make
-// that first call before any stream capture.  All calls share one workspace per device,
-// so calls that overlap on the GPU race; each call writes the whole [A | I] block and
-// the pivot slot before reading them, so nothing needs to start at zero.
+// Each call looks up the scratch address (cudaGetSymbolAddress) with the current device;
+// the first call on a device also loads this module there, so make that first call
+// before any stream capture.  All calls share one workspace per device, so calls that
+// overlap on the GPU race; each call writes the whole [A | I] block and the pivot slot
+// before reading them, so nothing needs to start at zero.  A singular input is not
+// detected: a zero pivot gives inf/NaN entries and the call still returns MSG_OK (the
+// work is queued, not awaited, so no status can come back from the device).
 MSG_API int msg_gpu_dense_inverse_noalloc(int32_t n, const double *a_dev, double *inv_dev, void *stream) {
   if (n < 1 || n > kNoAllocMaxN) {
     set_error("dense_inverse_noalloc: n = %d outside 1..%d (workspace limit)", (int)n, kNoAllocMaxN);
