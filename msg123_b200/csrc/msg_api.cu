@@ -883,6 +883,27 @@ int msg_gpu_calc_mass(msg_ctx_t *c, double *out9) {
   return MSG_OK;
 }
 
+int msg_gpu_cell_mass(msg_ctx_t *c, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
+                      double *riv, double *lak, double *drn) {
+  if (!c) return MSG_ERR_ARG;
+  const size_t N = c->N, S = c->S;
+  // Krylov scratch vectors (free between solves) hold the device copies
+  int rc = launch_cell_mass(c, c->r, c->rs, c->v, c->p, c->t, c->z);
+  if (rc) return rc;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  if (sto) MSG_CUDA(cudaMemcpy(sto, c->r, N * 8, cudaMemcpyDeviceToHost));
+  if (con) MSG_CUDA(cudaMemcpy(con, c->rs, N * 8, cudaMemcpyDeviceToHost));
+  if (sea) MSG_CUDA(cudaMemcpy(sea, c->v, N * 8, cudaMemcpyDeviceToHost));
+  if (rec) MSG_CUDA(cudaMemcpy(rec, c->p, S * 8, cudaMemcpyDeviceToHost));
+  if (sur) MSG_CUDA(cudaMemcpy(sur, c->t, S * 8, cudaMemcpyDeviceToHost));
+  if (drn) MSG_CUDA(cudaMemcpy(drn, c->z, S * 8, cudaMemcpyDeviceToHost));
+  // no wells, rivers or lakes exist in a context: their volumes are zero
+  if (wel) memset(wel, 0, N * 8);
+  if (riv) memset(riv, 0, S * 8);
+  if (lak) memset(lak, 0, S * 8);
+  return MSG_OK;
+}
+
 int msg_gpu_water_table(msg_ctx_t *c, double *wtable) {
   if (!c || !wtable) return MSG_ERR_ARG;
   int rc = launch_water_table(c, c->tmpv);   // tmpv: N >= S doubles of scratch

@@ -97,6 +97,8 @@ int launch_make_matvec(msg_ctx *c, bool reuse = false);
 // Export the DIA Jacobian into the reference CSR order.
 int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
 int launch_mass(msg_ctx *c, double *out9_dev);
+int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *rec, double *sur,
+                     double *drn);
 
 // ---- msg_linear.cu ----------------------------------------------------------------------------
 int build_wavefront(msg_ctx *c);

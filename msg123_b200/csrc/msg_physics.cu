@@ -422,54 +422,83 @@ __global__ void k_dia_to_csr(Geo g, const int *offind, const double *lu, double 
     if (has[d]) lumat[k++] = lu[(size_t)d * g.N + i];
 }
 
-// calc_mass (Calc_function.f90:103-174) terms x delt, block partial sums of
-// storage, flow, recharge, surface, sea and drainage.
+// calc_mass (Calc_function.f90:103-174) terms of cell i, each times delt: acc[0] storage
+// (func_stochn), acc[1] flow from the neighbours in CSR face order (func_connflow),
+// acc[2] recharge (func_rechterm), acc[3] surface (func_surfterm with surf_old), acc[4] sea
+// (func_sealterm: one sea face per top cell), acc[5] free drainage (extension).  acc[2..4]
+// belong to top cells, acc[5] to bottom cells; the others are zero.
+__device__ __forceinline__ void mass_terms(const FluxArgs &a, int i, const double *h_old, const double *s_old,
+                                           const double *s_new, const double *alp_new, const double *alp_old,
+                                           const float *poro, const double *vol, double delt_inv, double delt,
+                                           double acc[6]) {
+  const Geo g = a.g;
+  for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+  int ix, iy, iz;
+  cell_ijk(g, i, ix, iy, iz);
+  double hi = a.h[i], kri = a.kr[i];
+  double ch1 = __dmul_rn(__dmul_rn(alp_old[i], s_old[i]), h_old[i]);
+  double ch2 = __dmul_rn(__dmul_rn(alp_new[i], s_new[i]), hi);
+  double ch = __dadd_rn(__dsub_rn(ch2, ch1), __dmul_rn((double)poro[i], __dsub_rn(s_new[i], s_old[i])));
+  acc[0] = __dmul_rn(__dmul_rn(__dmul_rn(-ch, delt_inv), vol[i]), delt);
+  const int nbd[6] = {-g.nxy, -g.nx, -1, 1, g.nx, g.nxy};
+  const bool has[6] = {iz > 0, iy > 0, ix > 0, ix < g.nx - 1, iy < g.ny - 1, iz < g.nz - 1};
+  double cf = 0.0;
+  for (int d = 0; d < 6; ++d) {
+    if (!has[d]) continue;
+    int j = i + nbd[d];
+    size_t fi = (d < 3) ? (size_t)d * g.N + i : (size_t)(5 - d) * g.N + j;
+    double delhead = __dsub_rn(a.h[j], hi);
+    double relat = upwind(-delhead, kri, a.kr[j]);
+    cf = __dadd_rn(cf, __dmul_rn(__dmul_rn(__dmul_rn(a.hy[fi], relat), a.ab[fi]), delhead));
+  }
+  acc[1] = __dmul_rn(cf, delt);
+  if (iz == 0) {
+    double delh, over;
+    double sf = surf_term(hi, a.surf_head[i], a.surf_top[i], a.surf_bott[i], a.surf_reli[i], a.surf_parm[i],
+                          a.hydf_surf[i], a.abyd_surf[i], kri, delh, over);
+    acc[2] = __dmul_rn(a.calc_rech[i], delt);
+    acc[3] = __dmul_rn(sf, delt);
+    if (a.sea_top)
+      acc[4] = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(a.sea_hydf[i], kri), a.sea_abyd[i]), __dsub_rn(a.read_seal[i], hi)), delt);
+  }
+  if (a.free_drainage && iz == g.nz - 1) {
+    double coef = a.drain[i - (g.nz - 1) * g.nxy];
+    acc[5] = __dmul_rn(-__dmul_rn(coef, kri), delt);
+  }
+}
+
+// calc_mass summed over cells: block partial sums of the six terms.
 __global__ void __launch_bounds__(256) k_mass(FluxArgs a, const double *h_old, const double *s_old,
                                               const double *s_new, const double *alp_new, const double *alp_old,
                                               const float *poro, const double *vol, double delt_inv, double delt,
                                               double *part9) {
   __shared__ double sh[8];
-  const Geo g = a.g;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  if (i < g.N) {
-    int ix, iy, iz;
-    cell_ijk(g, i, ix, iy, iz);
-    double hi = a.h[i], kri = a.kr[i];
-    double ch1 = __dmul_rn(__dmul_rn(alp_old[i], s_old[i]), h_old[i]);
-    double ch2 = __dmul_rn(__dmul_rn(alp_new[i], s_new[i]), hi);
-    double ch = __dadd_rn(__dsub_rn(ch2, ch1), __dmul_rn((double)poro[i], __dsub_rn(s_new[i], s_old[i])));
-    acc[0] = __dmul_rn(__dmul_rn(__dmul_rn(-ch, delt_inv), vol[i]), delt);
-    const int nbd[6] = {-g.nxy, -g.nx, -1, 1, g.nx, g.nxy};
-    const bool has[6] = {iz > 0, iy > 0, ix > 0, ix < g.nx - 1, iy < g.ny - 1, iz < g.nz - 1};
-    double cf = 0.0;
-    for (int d = 0; d < 6; ++d) {
-      if (!has[d]) continue;
-      int j = i + nbd[d];
-      size_t fi = (d < 3) ? (size_t)d * g.N + i : (size_t)(5 - d) * g.N + j;
-      double delhead = __dsub_rn(a.h[j], hi);
-      double relat = upwind(-delhead, kri, a.kr[j]);
-      cf = __dadd_rn(cf, __dmul_rn(__dmul_rn(__dmul_rn(a.hy[fi], relat), a.ab[fi]), delhead));
-    }
-    acc[1] = __dmul_rn(cf, delt);
-    if (iz == 0) {
-      double delh, over;
-      double sf = surf_term(hi, a.surf_head[i], a.surf_top[i], a.surf_bott[i], a.surf_reli[i], a.surf_parm[i],
-                            a.hydf_surf[i], a.abyd_surf[i], kri, delh, over);
-      acc[2] = __dmul_rn(a.calc_rech[i], delt);
-      acc[3] = __dmul_rn(sf, delt);
-      if (a.sea_top)
-        acc[4] = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(a.sea_hydf[i], kri), a.sea_abyd[i]), __dsub_rn(a.read_seal[i], hi)), delt);
-    }
-    if (a.free_drainage && iz == g.nz - 1) {
-      double coef = a.drain[i - (g.nz - 1) * g.nxy];
-      acc[5] = __dmul_rn(-__dmul_rn(coef, kri), delt);
-    }
-  }
+  if (i < a.g.N) mass_terms(a, i, h_old, s_old, s_new, alp_new, alp_old, poro, vol, delt_inv, delt, acc);
   for (int q = 0; q < 6; ++q) {
     double s = block_sum<256>(acc[q], sh);
     if (threadIdx.x == 0) part9[(size_t)q * gridDim.x + blockIdx.x] = s;
   }
+}
+
+// calc_cell_mas (Calc_output.f90:54-91): the same terms per cell, in the reference's
+// arrays -- storage, flow and sea per cell [N]; recharge, surface and drainage per
+// surface column [S] (drainage leaves through the column's bottom cell).
+__global__ void __launch_bounds__(256) k_cell_mass(FluxArgs a, const double *h_old, const double *s_old,
+                                                   const double *s_new, const double *alp_new,
+                                                   const double *alp_old, const float *poro, const double *vol,
+                                                   double delt_inv, double delt, double *sto, double *con,
+                                                   double *sea, double *rec, double *sur, double *drn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.g.N) return;
+  double acc[6];
+  mass_terms(a, i, h_old, s_old, s_new, alp_new, alp_old, poro, vol, delt_inv, delt, acc);
+  sto[i] = acc[0];
+  con[i] = acc[1];
+  sea[i] = acc[4];
+  if (i < a.g.nxy) { rec[i] = acc[2]; sur[i] = acc[3]; }
+  if (i >= (a.g.nz - 1) * a.g.nxy) drn[i - (a.g.nz - 1) * a.g.nxy] = acc[5];
 }
 
 // ---------------------------------------------------------------------------------
@@ -646,6 +675,21 @@ int launch_mass(msg_ctx *c, double *out9_dev) {
   }
   MSG_CUDA(cudaMemcpyAsync(out9_dev, out, sizeof(out), cudaMemcpyHostToDevice, c->stream));
   MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *rec, double *sur, double *drn) {
+  // old-level vG (alp_old) into tmpv / kr_per scratch, then new-level into srat_new / kr / alp,
+  // as launch_mass does
+  double *alp_old = c->tmpv, *s_tmp = c->sto, *kr_tmp = c->kr_per;
+  int rc;
+  if ((rc = launch_srat_rperm(c, c->head_old, 0.0, s_tmp, kr_tmp, alp_old))) return rc;
+  if ((rc = launch_srat_rperm(c, c->head_new, 0.0, c->srat_new, c->kr, c->alp))) return rc;
+  FluxArgs a = flux_args(c, c->head_new);
+  a.surf_head = c->surf_old;
+  k_cell_mass<<<nblk(c->N), 256, 0, c->stream>>>(a, c->head_old, c->srat_old, c->srat_new, c->alp, alp_old, c->poro,
+                                                  c->cell_vol, c->delt_inv, c->delt, sto, con, sea, rec, sur, drn);
+  MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
 

@@ -293,6 +293,18 @@ class GpuSolver:
         _check(load_library().msg_gpu_calc_mass(self.h, dptr(out)), "calc_mass")
         return out
 
+    def cell_mass(self):
+        """calc_cell_mas (Calc_output.f90:54-91): the step's volumes per cell, dict of sto,
+        con, sea, wel [ncalc] and rec, sur, riv, lak, drn [ncals]."""
+        L = load_library()
+        L.msg_gpu_cell_mass.argtypes = [C.c_void_p] + [abi.PD] * 9
+        N, S = self.n, self.ncals
+        keys = (("sto", N), ("con", N), ("sea", N), ("wel", N), ("rec", S), ("sur", S), ("riv", S), ("lak", S),
+                ("drn", S))
+        out = {k: np.zeros(n) for k, n in keys}
+        _check(L.msg_gpu_cell_mass(self.h, *(dptr(out[k]) for k, _ in keys)), "cell_mass")
+        return out
+
     def amg_sizes(self):
         """(rows, off-diagonal entries, prolongation entries from the level above) of each
         level of the last AMG setup, level 0 = Jacobian (its prolongation count is 0)."""

@@ -1273,6 +1273,49 @@ static void calc_mass(orc_t *o, double *out9) {
   free(an); free(ao); free(so); free(kr); free(sf);
 }
 
+/* calc_cell_mas (Calc_output.f90:54-91): calc_mass (Calc_function.f90:103-174, sfla = 0)
+ * per cell instead of summed.  stom, conm, seam: [ncalc]; recm, surm, drn: [ncals] (drn:
+ * free-drainage outflow of each column's bottom cell, an extension).  Each term is the
+ * reference's rate times delt; seam accumulates over the sea faces of a cell
+ * (func_sealterm, Calc_function.f90:506-509) into an array zeroed by calc_cell_mas. */
+static void cell_mass(orc_t *o, double *stom, double *conm, double *seam, double *recm, double *surm,
+                      double *drn) {
+  int N = o->ncalc, S = o->ncals;
+  double *an = xc(N, sizeof(double)), *ao = xc(N, sizeof(double)), *so = xc(N, sizeof(double));
+  double *kr = xc(N, sizeof(double));
+  srat_rperm(o, DZERO, o->head_old, so, kr, ao);
+  srat_rperm(o, DZERO, o->head_new, o->srat_new, o->rel_perm, an);
+  for (int i = 0; i < N; ++i) {
+    double ch1 = ao[i] * o->srat_old[i] * o->head_old[i];
+    double ch2 = an[i] * o->srat_new[i] * o->head_new[i];
+    double ch = (ch2 - ch1) + (double)o->poro[i] * (o->srat_new[i] - o->srat_old[i]);
+    stom[i] = -ch * o->delt_inv * o->cell_vol[i] * o->delt;
+    double cf = DZERO;
+    for (int ind = o->offind[i]; ind < o->offind[i + 1]; ++ind) {
+      int j = o->offrow[ind];
+      double dh = o->head_new[j] - o->head_new[i];
+      double relat = hyd_upwind(-dh, o->rel_perm[i], o->rel_perm[j]);
+      cf = cf + o->sat_hydf[ind] * relat * o->area_dis[ind] * dh;
+    }
+    conm[i] = cf * o->delt;
+    seam[i] = DZERO;
+  }
+  for (int s = 0; s < S; ++s) drn[s] = DZERO;
+  for (int i = 0; i < N; ++i)
+    if (o->drain_coef[i] != DZERO) drn[i % S] = -(o->drain_coef[i] * o->rel_perm[i]) * o->delt;
+  func_surfterm(o, o->head_new, o->surf_old, surm);
+  for (int s = 0; s < S; ++s) { recm[s] = o->calc_rech[s] * o->delt; surm[s] = surm[s] * o->delt; }
+  double *flow = xc(o->nseal > 0 ? o->nseal : 1, sizeof(double));
+  for (int k = 0; k < o->nseal; ++k) {
+    int c = o->sea2cal[k], s = o->sea2sea[k];
+    double dh = o->read_seal[s] - o->head_new[c];
+    flow[k] = o->sea_hydf[k] * o->rel_perm[c] * o->sea_abyd[k] * dh;
+  }
+  for (int k = 0; k < o->nseal; ++k) seam[o->sea2cal[k]] = seam[o->sea2cal[k]] + flow[k];
+  for (int i = 0; i < N; ++i) seam[i] = seam[i] * o->delt;
+  free(an); free(ao); free(so); free(kr); free(flow);
+}
+
 /* =================================================================================
  * Exported API (ctypes), mirroring include/msg123_gpu.h entry points.
  * =================================================================================*/
@@ -1436,6 +1479,9 @@ int orc_advance(void *h, int nsteps, double rech_until, double rech_after, msg_r
 }
 
 void orc_calc_mass(void *h, double *out9) { calc_mass((orc_t *)h, out9); }
+void orc_cell_mass(void *h, double *sto, double *con, double *sea, double *rec, double *sur, double *drn) {
+  cell_mass((orc_t *)h, sto, con, sea, rec, sur, drn);
+}
 
 void orc_vecjacf(void *h, const double *x, const double *v, double *out) { calc_vecjacf((orc_t *)h, x, v, out); }
 

@@ -48,6 +48,7 @@ def lib():
         L.orc_init_state.argtypes = [vp, abi.PD, C.c_double]
         L.orc_set_state.argtypes = [vp, abi.PD, abi.PD, abi.PD, abi.PD, C.c_double]
         L.orc_srat_rperm.argtypes = [vp, abi.PD, C.c_double, abi.PD, abi.PD, abi.PD]
+        L.orc_cell_mass.argtypes = [vp] + [abi.PD] * 6
         L.orc_amg_level_sizes.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PI]
         L.orc_amg_level.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
         _lib = L
@@ -192,6 +193,14 @@ class Oracle:
     def calc_mass(self):
         out = np.zeros(9)
         lib().orc_calc_mass(C.c_void_p(self.h), dptr(out))
+        return out
+
+    def cell_mass(self):
+        """calc_cell_mas per cell: dict of sto, con, sea [ncalc] and rec, sur, drn [ncals]."""
+        N, S = self.prob.ncalc, self.prob.ncals
+        out = dict(sto=np.zeros(N), con=np.zeros(N), sea=np.zeros(N), rec=np.zeros(S), sur=np.zeros(S),
+                   drn=np.zeros(S))
+        lib().orc_cell_mass(C.c_void_p(self.h), *(dptr(out[k]) for k in ("sto", "con", "sea", "rec", "sur", "drn")))
         return out
 
     def counters(self):

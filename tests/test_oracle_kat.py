@@ -781,3 +781,28 @@ def test_reference_expressible_box():
     m = o.calc_mass()
     assert m[8] == 0.0 and m[7] > 0.0          # no drainage; inflow from the ponded layer
     assert abs(m[0] + m[1] + m[4] + m[7]) <= 1e-10 * m[7]       # measured 2.7e-12
+
+
+@pytest.mark.parametrize("name,kw", [("box", dict(shape=(5, 4, 7))), ("hetero", dict(shape=(8, 7, 6), seed=3))])
+def test_cell_mass_sums_to_calc_mass(name, kw):
+    """calc_cell_mas restated per cell: summed over cells in the same order, each array
+    gives calc_mass's whole-grid total bit for bit (storage, flow, drainage: cells in order;
+    recharge, surface: columns in order), and the sea volume lands in the top cells only."""
+    p = make_config(name, **kw)
+    o = Oracle(p)
+    o.init_state()
+    rc, _ = o.advance(nsteps=2)
+    assert rc == 0
+    cm = o.cell_mass()
+    tot = o.calc_mass()
+    seq = lambda a: float(np.add.accumulate(a)[-1]) if len(a) else 0.0
+    assert seq(cm["sto"]) == tot[0]
+    assert seq(cm["con"]) == tot[1]
+    assert seq(cm["rec"]) == tot[2]
+    assert seq(cm["sur"]) == tot[4]
+    assert abs(cm["sea"].sum() - tot[7]) <= 1e-14 * max(abs(tot[7]), 1e-300)
+    assert not np.any(cm["sea"][p.ncals:])
+    bottom = cm["drn"]
+    assert abs(bottom.sum() - tot[8]) <= 1e-13 * max(abs(tot[8]), 1e-300)
+    if not p.free_drainage:
+        assert not np.any(bottom)
