@@ -5,18 +5,28 @@ setup, BiCGStab, line search) over the whole grid.  The workload is the
 512x512x96 heterogeneous block (25,165,824 cells, sigma_lnK = 1.5, rain 20 mm/h,
 adaptive steps from 600 s, Newton tolerance 1e-8 relative head), synthetic and seeded.
 
-* value     : mixed precision + learned initial guess (FP32/BF16 V-cycle, FP64 Krylov and
-              Newton, AMG hierarchy rebuilt every 4 time steps, CNN guess with extrapolation
-              fallback); cells x accepted steps / device time of the K timed steps
-              (CUDA events on the library stream).
-* plain_fp64: the reference's method on the same field on the GPU (FP64 everywhere,
-              AMG rebuilt at every Newton iteration, Newton started from the previous
-              head), the path the north-star ratio is taken against.
-* e2e       : the mixed+learned path through the public C ABI with the state in host
-              memory (head/srat/surface copied in and out through set_state/get_state
-              every step).
-* cpu_baseline / --impl reference: the C restatement of the reference path (OpenMP,
-              all host cores) on a bounded block of the same generator.
+W warm-up steps run on the value path; every arm below then starts from that same saved
+time level (msg_gpu_copy_state) and covers the same window:
+
+* value        : mixed precision + learned initial guess (FP32/BF16 V-cycle, FP64 Krylov
+                 and Newton, AMG hierarchy rebuilt every 4 time steps, CNN guess with
+                 extrapolation fallback); cells x K accepted steps / device time (CUDA
+                 events on the library stream).  It ends at simulated time T.
+* arms         : the same window up to T with one change at a time -- mixed precision
+                 with the plain extrapolation (no network), FP64 with the extrapolation
+                 and the same AMG reuse, and plain FP64 (the reference's method on the
+                 GPU: AMG rebuilt at every Newton iteration, Newton from the previous
+                 head), each with Newton/Krylov counts, rejections and simulated seconds.
+                 The head and the stored water volume of the value path are compared with
+                 the plain FP64 arm at T.
+* e2e          : the value path over the same K steps through the public C ABI with the
+                 state in pinned host memory (set_state / advance / get_state each step,
+                 copies inside the timed region, host wall clock).
+* cpu_baseline : the C restatement of the reference path (OpenMP, all host cores) with
+                 the reference's own method (AMG preconditioner as the reference applies it,
+                 i.e. the level-1 DILU; FP64; previous-head start) on the 256x256x64
+                 heterogeneous block's first accepted steps; the GPU runs the same method on
+                 the same steps beside it.  --impl reference prints that CPU run as its line.
 
 Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (torchrun): every rank solves its own seeded realisation (independent
@@ -40,7 +50,8 @@ METRIC = "cell-timesteps/s at 1e-8 rel head tol"
 # the 256x256x64 block (dram__bytes_read.sum + dram__bytes_write.sum, both kernels) divided
 # by its 4,194,304 cells; traffic grows in proportion to the cells.
 TRAFFIC_CALC_FUNC_PER_CELL = 150.0
-TRAFFIC_SOURCE = "profiles/calc_func_kernels_hetero_256x256x64.md, scaled by cells"
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_cell<0> + k_flux_res on the "
+                  "256x256x64 block (150 B per cell), scaled by cells")
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 # Algorithmic bytes per cell of the kernels timed by msg_gpu_kernel_time (compulsory
@@ -96,9 +107,11 @@ def vcycle_bytes(sizes, sweeps, coarse_max):
     return total
 
 
-# Learned-guess CNN on the tensor cores: 4 convolutions x 27 taps x 16 x 16 (channels padded
-# to 16, as the tcgen05 MMA computes them) x 2 flops per cell.
-CNN_FLOP_PER_CELL = 4 * 27 * 16 * 16 * 2
+# Learned-guess CNN, algorithmic FLOPs per cell: 27 taps x 2 x (7 inputs x 16 + 16 x 16 +
+# 16 x 16 + 16 x 1 output) = 34,560.  The tensor cores compute every layer with 16 input and
+# 16 output channels (the zero-padded ones included): 55,296 issued FLOPs per cell.
+CNN_FLOP_PER_CELL = 27 * 2 * (7 * 16 + 16 * 16 + 16 * 16 + 16 * 1)
+CNN_FLOP_ISSUED_PER_CELL = 4 * 27 * 16 * 16 * 2
 
 
 def _peak_value(v):
@@ -211,11 +224,18 @@ def make_problem(args, rank):
     return make_config(args.workload, **kw)
 
 
-# learned guess used directly (no residual check: it costs two residual evaluations per step
-# and rarely rejects a guess in this window); a failed solve from it is redone from the
-# plain extrapolation
+# value path: mixed precision, learned guess used directly (a failed solve from it is redone
+# from the plain extrapolation), AMG hierarchy kept for 4 time steps, two-pow Mualem kr
 FAST = dict(precision=1, amg_lag=4, guess_mode=2, guess_select=0, vg_form=1)
-PLAIN = dict(precision=0, amg_lag=0, guess_mode=0)
+# one change at a time from the value path, over the same window
+ARMS = (("mixed_extrapolation", dict(FAST, guess_mode=1)),
+        ("fp64_extrapolation", dict(FAST, precision=0, guess_mode=1)),
+        ("plain_fp64", dict(precision=0, amg_lag=0, guess_mode=0, vg_form=0)))
+# the reference's own method: its AMG preconditioner as it acts (the level-1 DILU solve),
+# FP64, the reference's four-pow kr, Newton from the previous head
+REF_METHOD = dict(precon_type=1, ref_quirks=1, precision=0, amg_lag=0, guess_mode=0, vg_form=0)
+CPU_WORKLOAD = ("hetero", (256, 256, 64))
+CPU_STEPS = 4
 
 
 def workload_config(args, prob):
@@ -224,26 +244,87 @@ def workload_config(args, prob):
                         f"lnKs field, 20 mm/h rain, adaptive dt from {prm['ini_step']:.0f} s",
             "solver": "Newton (Eisenstat-Walker, cubic line search) + BiCGStab + smoothed-aggregation AMG",
             "value_path": "mixed precision (FP32 V-cycle, BF16 coarse operators, FP64 Krylov/Newton/coarse LU) + "
-                          "learned initial guess (used directly, extrapolation fallback), AMG hierarchy rebuilt every 4 "
-                          "time steps, two-pow form of Mualem kr (vg_form 1)",
-            "baseline_path": "plain FP64, AMG rebuilt every Newton iteration, Newton from the previous head",
+                          "learned initial guess (guess_select %d), AMG hierarchy rebuilt every %d time steps, "
+                          "two-pow form of Mualem kr (vg_form %d)" % (FAST["guess_select"], FAST["amg_lag"],
+                                                                      FAST["vg_form"]),
+            "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} after {args.warmup} warm-up steps of "
+                      "the value path; every arm starts from the same saved time level",
             "newton_tol": "max|dh| <= 1e-8 max|h|",
             "l2": "inputs larger than L2 (126 MB); no flush needed",
             "parallelism": f"replicas x{args.gpus}",
             **({"overrides": dict(kv.split("=", 1) for kv in args.set)} if args.set else {})}
 
 
-def timed_advance(g, steps):
+def arm_stats(prob, st, ms, dist, fallbacks=None):
+    """Whole-job figures of one arm: value, counts per accepted step, simulated time."""
+    acc = max(st["accepted"], 1)
+    tmax = reduce(dist, ms, "max")
+    out = {"value": reduce(dist, float(prob.ncalc * st["accepted"]), "sum") / (tmax * 1e-3),
+           "ms_per_step": tmax / acc, "accepted": st["accepted"], "rejected": st["rejected"],
+           "newton_per_step": st["newton_total"] / acc, "krylov_per_step": st["krylov_total"] / acc,
+           "backtracks": st["back_total"], "simulated_s": st["current_t"],
+           "simulated_s_per_s": None}
+    if fallbacks is not None:
+        out["guess_fallbacks"], out["guess_rejected"] = fallbacks
+    return out
+
+
+def water_volume(g, head):
+    """Stored water of a state, sum over cells of vol * (theta_s S + alpha_ss S h) -- the
+    quantity whose change calc_mass books as storage (Calc_function.f90:176-210)."""
+    p = g.prob
+    srat, _, sstor = g.srat_rperm(head)
+    return float(np.sum(p.cell_vol * (p.poro.astype(np.float64) * srat + sstor * srat * head)))
+
+
+def inflow_volume(prob, t0, t1):
+    """Recharge volume entering between simulated times t0 and t1 (rain until rech_until)."""
+    ru = prob.rech_until
+    wet = max(min(t1, ru) - min(t0, ru), 0.0)
+    dry = max(t1 - max(t0, ru), 0.0)
+    return float(np.sum(prob.rech)) * (wet + prob.rech_after * dry)
+
+
+def prep_arm(prob, kw, src, cnn, end_time=None):
+    """A fresh context with settings kw, started from src's time level (the network
+    attached when kw asks for the learned guess)."""
+    from msg123_b200.solver import GpuSolver
+    extra = {} if end_time is None else {"end_time": end_time}
+    g = GpuSolver(prob, **kw, **extra)
+    if kw.get("guess_mode") == 2:
+        cnn.attach(g)
+    g.copy_state_from(src)
+    return g
+
+
+def run_arm(g, steps):
+    """Advance by `steps` accepted steps (or to the context's end time): (stats, device ms,
+    (learned guesses redone from the extrapolation, learned guesses not used))."""
     rc, st = g.advance(nsteps=steps)
-    return st, g.timers()["total_ms"]
+    return st, g.timers()["total_ms"], (g.guess_fallbacks(), g.guess_rejected())
 
 
-def cpu_run(prob, budget_s, max_steps):
-    """Oracle (C restatement, OpenMP) on the plain FP64 path, bounded in time."""
+def cpu_hw():
+    """CPU model, logical CPUs and the OpenMP thread count of this host."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count(), "omp_num_threads": int(os.environ.get("OMP_NUM_THREADS", "0"))}
+
+
+def cpu_run(prob, budget_s, max_steps, keep_state=False):
+    """Oracle (C restatement, OpenMP, all host cores) with the reference's method, bounded in
+    time: accepted steps from the initial state until max_steps or the budget."""
     from oracle.oracle import Oracle
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    o = Oracle(prob, **PLAIN)
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    threads = int(os.environ["OMP_NUM_THREADS"])
+    o = Oracle(prob, **REF_METHOD)
     o.init_state()
     steps, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < budget_s and steps < max_steps:
@@ -252,29 +333,43 @@ def cpu_run(prob, budget_s, max_steps):
             break
         steps += 1
     dt = time.perf_counter() - t0
+    head = o.get_state()["head_new"] if keep_state else None
     o.close()
-    return prob.ncalc * max(steps, 1) / dt, steps, dt, threads
+    return prob.ncalc * max(steps, 1) / dt, steps, dt, threads, head
 
 
 def cpu_sample_problem(args):
     from msg123_b200.config import make_config
-    return make_config(args.workload, shape=tuple(int(v) for v in args.cpu_shape.split("x")), seed=2024)
+    name, shape = CPU_WORKLOAD
+    if args.cpu_shape:
+        shape = tuple(int(v) for v in args.cpu_shape.split("x"))
+    return make_config(name, shape=shape, seed=2024)
+
+
+def cpu_sample_text(prob, steps, dt, threads):
+    return (f"first {steps} accepted step(s) of the {prob.nx}x{prob.ny}x{prob.nz} heterogeneous block "
+            f"(seed 2024, hydrostatic start, dt from 600 s) with the reference's method (AMG preconditioner "
+            f"as the reference applies it = level-1 DILU, FP64, Newton from the previous head), C restatement "
+            f"oracle/msg123_oracle.c, OpenMP {threads} threads, {dt:.1f} s")
 
 
 def run_reference(args):
     rank, ws, dist = dist_setup()
     if rank == 0:
         prob = cpu_sample_problem(args)
-        val, steps, dt, threads = cpu_run(prob, budget_s=60.0, max_steps=max(1, args.steps))
-        sample = (f"{steps} accepted step(s) of a {prob.nx}x{prob.ny}x{prob.nz} block of the same generator "
-                  f"(plain FP64 path), C restatement oracle/msg123_oracle.c with OpenMP, {dt:.1f} s")
+        val, steps, dt, threads, _ = cpu_run(prob, budget_s=150.0, max_steps=min(max(1, args.steps), CPU_STEPS))
+        cfg = {"workload": f"hetero {prob.nx}x{prob.ny}x{prob.nz} ({prob.ncalc} cells), heterogeneous lnKs "
+                           "field, 20 mm/h rain, adaptive dt from 600 s",
+               "path": "the reference's method (FP64, AMG preconditioner as applied by the reference, "
+                       "previous-head start) on the host cores",
+               "why_not_the_gpu_workload": "one step of the 25.2M-cell block takes about a minute on the host "
+                                           "cores; the 256x256x64 block's first steps are the planned sample",
+               **cpu_hw()}
         line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "cell-timesteps/s", "n_gpus": ws,
                 "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / max(steps, 1), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"{args.workload} generator, {prob.nx}x{prob.ny}x{prob.nz} block",
-                           "path": "plain FP64 (reference method)"},
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
                 "cpu_baseline": {"value": val, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
-                                 "sample": sample},
+                                 "sample": cpu_sample_text(prob, steps, dt, threads)},
                 "e2e": {"value": val, "unit": "cell-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -284,16 +379,15 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "hetero", "box"])
     ap.add_argument("--shape", default="")
-    ap.add_argument("--cpu-shape", default="96x96x96")
-    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--cpu-shape", default="")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-arms", action="store_true")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="override a solver parameter of the value path (e.g. amg_lag=8)")
     args = ap.parse_args()
@@ -314,95 +408,125 @@ def main():
     from msg123_b200.train_guess import load
     prob = make_problem(args, rank)
     cnn = load(Cnn(seed=0))
+    K = args.steps
 
-    # ---- mixed precision + learned guess: the headline -------------------------------
-    g = GpuSolver(prob, **FAST)
-    cnn.attach(g)
-    g.init_state()
-    g.advance(nsteps=args.warmup)
+    # ---- warm-up on the value path; its time level is where every arm starts -----------
+    gw = GpuSolver(prob, **FAST)
+    cnn.attach(gw)
+    gw.init_state()
+    _, stw = gw.advance(nsteps=args.warmup)
+    t_start = stw["current_t"]
+    barrier(dist)
+
+    # ---- value: mixed precision + learned guess, K accepted steps -------------------------
+    ga = prep_arm(prob, FAST, gw, cnn)
     barrier(dist)
     l0 = launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        st, ms = timed_advance(g, args.steps)
+        st, ms, fb = run_arm(ga, K)
     launches = launch_count() - l0
-    tmax = reduce(dist, ms, "max")
-    value = reduce(dist, float(prob.ncalc * st["accepted"]), "sum") / (tmax * 1e-3)
+    value_arm = arm_stats(prob, st, ms, dist, fb)
+    value = value_arm["value"]
+    tmax = value_arm["ms_per_step"] * max(st["accepted"], 1)
+    t_end = st["current_t"]
+    head_a = ga.get_state(out={"head_new": np.zeros(prob.ncalc)})["head_new"]
+    vol_a = water_volume(ga, head_a)
 
     # kernel timings for the roofline (state of the last timed step, library stream)
     hbm, tc_peak, src = load_peaks()
-    # the V-cycle first: make_matvec below re-assembles at the converged head, whose
-    # right-hand side is far smaller than any the solve passes to the preconditioner
-    t_prec = g.kernel_time(3, reps=5)
-    vc_bytes = vcycle_bytes(g.amg_sizes(), g.params["amg_sweeps"], g.params["amg_coarse_max"])
+    t_prec = ga.kernel_time(3, reps=5)
+    vc_bytes = vcycle_bytes(ga.amg_sizes(), ga.params["amg_sweeps"], ga.params["amg_coarse_max"])
     vc_gbs = vc_bytes / (t_prec * 1e-3) / 1e9
-    kt = {w: g.kernel_time(w, reps=10) for w in (0, 1, 2)}
+    kt = {w: ga.kernel_time(w, reps=10) for w in (0, 1, 2)}
     gbs = {w: ALG_BYTES[w] * prob.ncalc / (kt[w] * 1e-3) / 1e9 for w in kt}
-    t_setup = g.kernel_time(4, reps=2)
-    t_cnn = g.kernel_time(5, reps=5)
+    t_setup = ga.kernel_time(4, reps=2)
+    t_cnn = ga.kernel_time(5, reps=5)
     cnn_tflops = CNN_FLOP_PER_CELL * prob.ncalc / (t_cnn * 1e-3) / 1e12
+    ga.close()
 
-    # end to end through the public API, state in host memory
+    # ---- the other arms over the same window (to the value path's end time T) -------------
+    arms, errors = {}, None
+    if not args.no_arms:
+        for name, kw in ARMS:
+            barrier(dist)
+            g = prep_arm(prob, kw, gw, cnn, end_time=t_end)
+            sta, msa, _ = run_arm(g, 4 * K)
+            arms[name] = arm_stats(prob, sta, msa, dist)
+            if name == "plain_fp64":
+                head_d = g.get_state(out={"head_new": np.zeros(prob.ncalc)})["head_new"]
+                vol_d = water_volume(g, head_d)
+                inflow = inflow_volume(prob, t_start, t_end)
+                errors = {"against": "plain_fp64 at the same simulated time",
+                          "simulated_s": sta["current_t"],
+                          "head_rel": reduce(dist, float(np.max(np.abs(head_a - head_d)) / np.max(np.abs(head_d))),
+                                             "max"),
+                          "stored_water_rel_inflow": reduce(dist, abs(vol_a - vol_d) / inflow, "max"),
+                          "inflow_volume": inflow}
+            g.close()
+    for a in list(arms.values()) + [value_arm]:
+        a["simulated_s_per_s"] = (a["simulated_s"] - t_start) / (a["ms_per_step"] * max(a["accepted"], 1) * 1e-3)
+
+    # ---- end to end through the public API, state in pinned host memory -------------------
     e2e = None
     if not args.no_e2e:
         import torch
         N, S = prob.ncalc, prob.ncals
-        # state in pinned host memory, copied in and out through the public C ABI every step
-        pin = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-               for k, n in (("head_new", N), ("head_old", N), ("srat_new", N), ("srat_old", N), ("surf_head", S))}
-        g.get_state(out=pin)
+        ge = prep_arm(prob, FAST, gw, cnn)
+        pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+        heads = [pin(N), pin(N)]                    # [current, previous]: swapped, never copied
+        sat, surf = pin(N), pin(S)
+        ge.get_state(out={"head_new": heads[0], "head_old": heads[1], "srat_new": sat, "surf_head": surf})
         barrier(dist)
+        acc = newton = 0
         t0 = time.perf_counter()
-        acc = 0
-        for _ in range(args.steps):
-            g.set_state(head_new=pin["head_new"], head_old=pin["head_old"], srat_old=pin["srat_old"],
-                        surf_head=pin["surf_head"])
-            rc2, st2 = g.advance(nsteps=1)
-            g.get_state(out=pin)
-            pin["srat_old"][:] = pin["srat_new"]
+        for _ in range(K):
+            ge.set_state(head_new=heads[0], head_old=heads[1], srat_old=sat, surf_head=surf)
+            rc2, st2 = ge.advance(nsteps=1)
+            ge.get_state(out={"head_new": heads[1], "srat_new": sat, "surf_head": surf})
+            heads.reverse()
             acc += st2["accepted"]
+            newton += st2["newton_total"]
         te = reduce(dist, time.perf_counter() - t0, "max")
         e2e = {"value": reduce(dist, float(prob.ncalc * acc), "sum") / te, "unit": "cell-timesteps/s",
-               "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 4 * N * 8 + S * 8,
-               "path": "mixed + learned through msg_gpu_set_state / msg_gpu_advance / msg_gpu_get_state, "
-                       "pinned host buffers"}
-    g.close()
+               "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 2 * N * 8 + S * 8,
+               "accepted": acc, "newton_per_step": newton / max(acc, 1), "simulated_s": st2["current_t"],
+               "same_window_as_value": bool(acc == st["accepted"] and st2["current_t"] == t_end),
+               "path": "value path through msg_gpu_set_state (head_new, head_old, srat_old, surf_head) / "
+                       "msg_gpu_advance / msg_gpu_get_state (head_new, srat_new, surf_head), pinned host "
+                       "buffers, host wall clock"}
+        ge.close()
+    gw.close()
 
-    # ---- plain FP64 reference method on the same field ----------------------------------
-    plain = None
-    if not args.no_plain:
-        gp = GpuSolver(prob, **PLAIN)
-        gp.init_state()
-        gp.advance(nsteps=1)
-        barrier(dist)
-        stp, msp = timed_advance(gp, args.plain_steps)
-        tpm = reduce(dist, msp, "max")
-        pv = reduce(dist, float(prob.ncalc * stp["accepted"]), "sum") / (tpm * 1e-3)
-        plain = {"value": pv, "ms_per_step": tpm / max(stp["accepted"], 1),
-                 "newton_per_step": stp["newton_total"] / max(stp["accepted"], 1),
-                 "krylov_per_step": stp["krylov_total"] / max(stp["accepted"], 1),
-                 "steps": stp["accepted"], "simulated_s_per_step": None,
-                 "speedup_of_value": value / pv}
-        gp.close()
-
-    cpu = None
+    # ---- CPU baseline: the reference's method on the host cores, and on the GPU beside it --
+    cpu, refgpu = None, None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cp = cpu_sample_problem(args)
-        val, steps, dt, threads = cpu_run(cp, budget_s=25.0, max_steps=args.steps)
+        val, steps, dt, threads, head_c = cpu_run(cp, budget_s=60.0, max_steps=CPU_STEPS, keep_state=True)
         cpu = {"value": val, "unit": "cell-timesteps/s", "cores": threads, "kind": "port",
-               "sample": f"{steps} accepted step(s) of a {cp.nx}x{cp.ny}x{cp.nz} block of the same generator on the "
-                         f"plain FP64 path, C restatement oracle/msg123_oracle.c with OpenMP ({dt:.1f} s)"}
+               "sample": cpu_sample_text(cp, steps, dt, threads), **cpu_hw()}
+        gr = GpuSolver(cp, **REF_METHOD)
+        gr.init_state()
+        rcr, str_ = gr.advance(nsteps=steps)
+        head_g = gr.get_state(out={"head_new": np.zeros(cp.ncalc)})["head_new"]
+        refgpu = {"workload": f"hetero {cp.nx}x{cp.ny}x{cp.nz}", "steps": str_["accepted"],
+                  "value": cp.ncalc * str_["accepted"] / (gr.timers()["total_ms"] * 1e-3),
+                  "newton_per_step": str_["newton_total"] / max(str_["accepted"], 1),
+                  "speedup_over_cpu": cp.ncalc * str_["accepted"] / (gr.timers()["total_ms"] * 1e-3) / val,
+                  "head_rel_vs_cpu": float(np.max(np.abs(head_g - head_c)) / np.max(np.abs(head_c)))}
+        gr.close()
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "cell-timesteps/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": tmax / max(st["accepted"], 1), "higher_is_better": True,
+            "metric": METRIC, "value": value, "unit": "cell-timesteps/s", "n_gpus": ws, "steps": K,
+            "warmup": args.warmup, "ms_per_step": value_arm["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 (Krylov/Newton) + f32/bf16 (V-cycle)",
             "data": "synthetic (seeded lnKs field and van Genuchten draws)", "config": workload_config(args, prob),
-            "newton": {"accepted": st["accepted"], "rejected": st["rejected"],
-                       "newton_per_step": st["newton_total"] / max(st["accepted"], 1),
-                       "krylov_per_step": st["krylov_total"] / max(st["accepted"], 1),
-                       "backtracks": st["back_total"], "simulated_s": st["current_t"]},
-            "plain_fp64": plain,
+            "newton": {k: value_arm[k] for k in ("accepted", "rejected", "newton_per_step", "krylov_per_step",
+                                                 "backtracks", "simulated_s", "guess_fallbacks", "guess_rejected")},
+            "window_start_s": t_start,
+            "arms": dict(arms, value=value_arm) if arms else None,
+            "speedup_over_plain_fp64": (value / arms["plain_fp64"]["value"]) if arms else None,
+            "errors_vs_fp64": errors,
             "roofline": {"kernel": KERNEL_NAMES[1], "bound": "hbm", "achieved": gbs[1], "peak": hbm,
                          "unit": "GB/s", "frac": gbs[1] / hbm, "peak_source": src,
                          "alg_bytes_per_cell": ALG_BYTES[1], "cells_per_launch": prob.ncalc,
@@ -412,12 +536,15 @@ def main():
                                          for w in (0, 2)},
                                         **{"learned-guess CNN, 4 tcgen05 convolutions": {
                                             "ms": t_cnn, "TFLOP/s": cnn_tflops, "frac": cnn_tflops / tc_peak,
-                                            "bound": "tensor", "peak_TFLOP/s": tc_peak},
+                                            "bound": "tensor", "peak_TFLOP/s": tc_peak,
+                                            "flop_per_cell": CNN_FLOP_PER_CELL,
+                                            "issued_TFLOP/s": CNN_FLOP_ISSUED_PER_CELL * prob.ncalc / (t_cnn * 1e-3) / 1e12},
                                            "mixed V-cycle, all levels": {
                                             "ms": t_prec, "GB/s": vc_gbs, "frac": vc_gbs / hbm,
                                             "alg_bytes": vc_bytes}}),
                          "vcycle_mixed_ms": t_prec, "amg_setup_ms": t_setup},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+            "cpu_baseline": cpu, "reference_method_gpu": refgpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     cnn.close()

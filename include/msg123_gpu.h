@@ -168,6 +168,14 @@ MSG_API int msg_gpu_get_connect(msg_ctx_t *ctx, int32_t *offind, int32_t *offrow
  * then the rollback point of the next step as in the reference. */
 MSG_API int msg_gpu_set_state(msg_ctx_t *ctx, const double *head_new, const double *head_old,
                       const double *srat_old, const double *surf_head, double delt);
+/* Copy the whole time level of src into dst, two contexts of the same grid on the same
+ * device: heads and saturations of both time levels, the level before them (the linear
+ * extrapolation and the learned guess read it), surface heads, recharge, the clock, delt
+ * and the step history apply_heuri and the guesses use.  Solver settings, the AMG
+ * hierarchy (rebuilt at dst's next Newton iteration) and the counters stay dst's own.
+ * So several settings can advance from one state, e.g. to compare them over the same
+ * window.  No counterpart in the reference, whose time level lives in module globals. */
+MSG_API int msg_gpu_copy_state(msg_ctx_t *dst, const msg_ctx_t *src);
 MSG_API int msg_gpu_get_state(msg_ctx_t *ctx, double *head_new, double *head_old, double *srat_new,
                       double *srat_old, double *surf_head);
 

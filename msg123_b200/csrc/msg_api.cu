@@ -665,6 +665,29 @@ int msg_gpu_set_state(msg_ctx_t *c, const double *head_new, const double *head_o
   return MSG_OK;
 }
 
+int msg_gpu_copy_state(msg_ctx_t *dst, const msg_ctx_t *src) {
+  if (!dst || !src) { set_error("copy_state: null context"); return MSG_ERR_ARG; }
+  if (dst->nx != src->nx || dst->ny != src->ny || dst->nz != src->nz) {
+    set_error("copy_state: grids differ (%dx%dx%d vs %dx%dx%d)", dst->nx, dst->ny, dst->nz, src->nx, src->ny, src->nz);
+    return MSG_ERR_SIZE;
+  }
+  if (dst->device != src->device) { set_error("copy_state: contexts on different devices"); return MSG_ERR_ARG; }
+  const size_t N = dst->N, S = dst->S;
+  MSG_CUDA(cudaStreamSynchronize(src->stream));
+  struct { double *d; const double *s; size_t n; } cp[] = {
+      {dst->head_new, src->head_new, N}, {dst->head_old, src->head_old, N}, {dst->head_old2, src->head_old2, N},
+      {dst->srat_new, src->srat_new, N}, {dst->srat_old, src->srat_old, N}, {dst->surf_head, src->surf_head, S},
+      {dst->surf_old, src->surf_old, S}, {dst->calc_rech, src->calc_rech, S}, {dst->rech_base, src->rech_base, S}};
+  for (auto &q : cp)
+    MSG_CUDA(cudaMemcpyAsync(q.d, q.s, q.n * 8, cudaMemcpyDeviceToDevice, dst->stream));
+  dst->current_t = src->current_t;
+  dst->delt = src->delt; dst->delt_inv = src->delt_inv;
+  dst->delt_old1 = src->delt_old1; dst->delt_old2 = src->delt_old2;
+  dst->timestep_num = src->timestep_num; dst->last_conv = src->last_conv; dst->last_out = src->last_out;
+  MSG_CUDA(cudaStreamSynchronize(dst->stream));
+  return MSG_OK;
+}
+
 int msg_gpu_get_state(msg_ctx_t *c, double *head_new, double *head_old, double *srat_new, double *srat_old,
                       double *surf_head) {
   if (!c) return MSG_ERR_ARG;

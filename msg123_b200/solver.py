@@ -169,20 +169,25 @@ class GpuSolver:
         _check(load_library().msg_gpu_set_state(self.h, *(dptr(a) for a in arrs), C.c_double(delt)), "set_state")
 
     def get_state(self, out=None):
-        """Copy the state to host arrays (new float64 arrays, or the C-contiguous float64
-        arrays of `out`, e.g. views of pinned memory)."""
+        """Copy the state to host arrays: new float64 arrays of all five fields, or the
+        fields named in `out` (C-contiguous float64 arrays, e.g. views of pinned memory);
+        fields missing from `out` are not copied."""
         N, S = self.n, self.ncals
+        sizes = (("head_new", N), ("head_old", N), ("srat_new", N), ("srat_old", N), ("surf_head", S))
         if out is None:
-            out = dict(head_new=np.zeros(N), head_old=np.zeros(N), srat_new=np.zeros(N), srat_old=np.zeros(N),
-                       surf_head=np.zeros(S))
-        for k, n in (("head_new", N), ("head_old", N), ("srat_new", N), ("srat_old", N), ("surf_head", S)):
-            a = out[k]
-            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n:
+            out = {k: np.zeros(n) for k, n in sizes}
+        for k, n in sizes:
+            a = out.get(k)
+            if a is not None and (a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n):
                 raise ValueError(f"get_state: {k} must be a C-contiguous float64 array of {n}")
-        _check(load_library().msg_gpu_get_state(self.h, *(dptr(out[k]) for k in
-                                                         ("head_new", "head_old", "srat_new", "srat_old",
-                                                          "surf_head"))), "get_state")
+        _check(load_library().msg_gpu_get_state(self.h, *(dptr(out.get(k)) for k, _ in sizes)), "get_state")
         return out
+
+    def copy_state_from(self, other):
+        """Take the whole time level of another context of the same grid (msg_gpu_copy_state)."""
+        L = load_library()
+        L.msg_gpu_copy_state.argtypes = [C.c_void_p, C.c_void_p]
+        _check(L.msg_gpu_copy_state(self.h, other.h), "copy_state")
 
     def water_table(self):
         """calc_wtable of the current state (Calc_output.f90:20-52): [ncals] heads,

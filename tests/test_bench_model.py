@@ -76,17 +76,25 @@ def test_load_peaks(tmp_path):
 
 class _FakeSolver:
     """Stands in for GpuSolver in a dry run of bench.main: fixed kernel times, one AMG level
-    pair, a state of the right size."""
+    pair, a state of the right size, a clock that stops at the context's end time."""
 
     def __init__(self, prob, **kw):
         self.prob, self.params = prob, dict(prob.params, **kw)
+        self.t = 0.0
 
     def init_state(self):
         pass
 
+    def copy_state_from(self, other):
+        self.t = other.t
+
     def advance(self, nsteps=1, **kw):
-        return 0, dict(accepted=nsteps, rejected=0, newton_total=5 * nsteps, krylov_total=5 * nsteps,
-                       back_total=0, current_t=600.0 * nsteps, delt=600.0, status=0)
+        n = 0
+        while n < nsteps and self.t < self.params["end_time"]:
+            self.t = min(self.t + 600.0, self.params["end_time"])
+            n += 1
+        return 0, dict(accepted=n, rejected=0, newton_total=5 * n, krylov_total=5 * n,
+                       back_total=0, current_t=self.t, delt=600.0, status=0)
 
     def timers(self):
         return {"total_ms": 10.0}
@@ -99,18 +107,33 @@ class _FakeSolver:
         return [(n, 6 * n, 0), (n // 8, n, n)]
 
     def get_state(self, out=None):
+        import numpy as np
+        out = out if out is not None else {}
+        for k, a in out.items():
+            a[:] = np.asarray(self.prob.head0 if k.startswith("head") else 0.5)[:a.size] if k.startswith("head") \
+                else 0.5
         return out
 
     def set_state(self, **kw):
         pass
 
+    def srat_rperm(self, head):
+        import numpy as np
+        return np.full(head.size, 0.5), np.ones(head.size), np.zeros(head.size)
+
+    def guess_fallbacks(self):
+        return 0
+
+    def guess_rejected(self):
+        return 0
+
     def close(self):
         pass
 
 
-@pytest.mark.parametrize("extra", [["--no-cpu", "--no-plain", "--no-e2e"],
-                                   ["--cpu-shape", "8x8x4", "--plain-steps", "2", "--no-e2e"],
-                                   ["--no-cpu", "--no-plain"]])
+@pytest.mark.parametrize("extra", [["--no-cpu", "--no-arms", "--no-e2e"],
+                                   ["--cpu-shape", "8x8x4", "--no-e2e"],
+                                   ["--no-cpu", "--no-arms"]])
 def test_bench_main_dry_run(monkeypatch, capsys, extra):
     """bench.main on the CPU with stand-ins for the CUDA solver and the network: the JSON
     line carries every key of the contract, with values derived from the stand-ins."""
@@ -138,14 +161,21 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
     assert r["ms_per_launch"] == 0.02 and r["unit"] == "GB/s" and 0 < r["frac"]
     assert r["others"]["mixed V-cycle, all levels"]["ms"] == 0.05
     assert r["vcycle_mixed_ms"] == 0.05 and line["config"]["workload"].startswith("hetero 8x8x4")
+    assert line["newton"]["accepted"] == 2 and line["newton"]["simulated_s"] == 3000.0 and line["window_start_s"] == 1800.0
+    if "--no-arms" not in extra:                      # every arm stops at the value path's end time
+        for name in ("mixed_extrapolation", "fp64_extrapolation", "plain_fp64", "value"):
+            assert line["arms"][name]["simulated_s"] == 3000.0
+        assert line["errors_vs_fp64"]["head_rel"] == 0.0
+        assert line["speedup_over_plain_fp64"] == pytest.approx(1.0)
     if "--no-e2e" not in extra:                       # pinned host state in and out every step
         e = line["e2e"]
-        assert e["h2d_bytes_per_step"] == 3 * 256 * 8 + 64 * 8 and e["d2h_bytes_per_step"] == 4 * 256 * 8 + 64 * 8
-        assert e["value"] > 0
+        assert e["h2d_bytes_per_step"] == 3 * 256 * 8 + 64 * 8 and e["d2h_bytes_per_step"] == 2 * 256 * 8 + 64 * 8
+        assert e["value"] > 0 and e["accepted"] == 2 and e["same_window_as_value"]
     if "--no-cpu" not in extra:                       # the oracle really ran on the 8x8x4 sample
         cb = line["cpu_baseline"]
         assert cb["kind"] == "port" and cb["value"] > 0 and "8x8x4" in cb["sample"]
-        assert line["plain_fp64"]["ms_per_step"] == pytest.approx(5.0)
+        assert cb["nproc"] >= 1 and "cpu_model" in cb
+        assert line["reference_method_gpu"]["steps"] >= 1
 
 
 def _bench_rank(rank, world, port, q):
@@ -161,7 +191,7 @@ def _bench_rank(rank, world, port, q):
     learned.Cnn = lambda seed=0: type("C", (), {"attach": lambda s, g: None, "close": lambda s: None})()
     train_guess.load = lambda c: c
     sys.argv = ["bench.py", "--workload", "hetero", "--shape", "8x8x4", "--steps", "2", "--warmup", "3",
-                "--gpus", str(world), "--no-cpu", "--no-plain", "--no-e2e"]
+                "--gpus", str(world), "--no-cpu", "--no-arms", "--no-e2e"]
     out = io.StringIO()
     with contextlib.redirect_stdout(out):
         bench.main()
