@@ -120,6 +120,10 @@ module msg_gpu
       import; type(c_ptr), value :: ctx
       real(c_double), intent(out) :: sto(*), con(*), sea(*), wel(*), rec(*), sur(*), riv(*), lak(*), drn(*)
     end function
+    ! calc_outvelc: facev(ncalc, 6) and pointv(ncalc, 3) in the layout of facev / pointv
+    integer(c_int) function msg_gpu_velocity(ctx, facev, pointv) bind(C)
+      import; type(c_ptr), value :: ctx; real(c_double), intent(out) :: facev(*), pointv(*)
+    end function
     integer(c_int) function msg_gpu_water_table(ctx, wtable) bind(C)
       import; type(c_ptr), value :: ctx; real(c_double), intent(out) :: wtable(*)
     end function

@@ -239,6 +239,14 @@ MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
  * come back zero.  Any pointer may be NULL. */
 MSG_API int msg_gpu_cell_mass(msg_ctx_t *ctx, double *sto, double *con, double *sea, double *wel, double *rec,
                               double *sur, double *riv, double *lak, double *drn);
+/* calc_outvelc (Calc_output.f90:168-241) at the current head_new (relative permeability
+ * recomputed there): facev [6*ncalc], face-major (facev[d*ncalc + i], d = up, north, west,
+ * east, south, down), the Darcy velocity through each face, positive into the cell,
+ * nondimensional like the reference's; pointv [3*ncalc] (x, y, z components, upward z
+ * positive), the cell-centred velocity the reference writes.  Faces with no connection are
+ * 0; under free drainage (extension) the bottom face of the lowest layer carries the
+ * unit-gradient outflow -Ksz*kr.  Either pointer may be NULL. */
+MSG_API int msg_gpu_velocity(msg_ctx_t *ctx, double *facev, double *pointv);
 /* Water table of the current state (calc_wtable, Calc_output.f90:20-52, called by
  * write_out_wtabf with head_new and srat_new): for each surface column, the head of the
  * lowest cell that is not fully saturated (srat != 1), scanning up from the bottom layer;

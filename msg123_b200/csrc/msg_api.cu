@@ -562,7 +562,7 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
   for (int k = 0; k < 6; ++k) { ALLOC(*fp[k], N * 4); UPLOAD(*fp[k], fs[k], N * 4); }
   ALLOC(c->cell_top, N * 8); UPLOAD(c->cell_top, g->cell_top, N * 8);
   ALLOC(c->cell_vol, N * 8); UPLOAD(c->cell_vol, g->cell_vol, N * 8);
-  ALLOC(c->hy, 3 * N * 8); ALLOC(c->ab, 3 * N * 8);
+  ALLOC(c->hy, 3 * N * 8); ALLOC(c->ab, 3 * N * 8); ALLOC(c->invd, 3 * N * 8);
   double **sp[] = {&c->surf_top, &c->surf_bott, &c->surf_reli, &c->surf_parm, &c->read_seal};
   const double *ss_[] = {g->surf_top, g->surf_bott, g->surf_reli, g->surf_parm, g->sea_head};
   for (int k = 0; k < 5; ++k) {
@@ -571,7 +571,7 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
     else MSG_CUDA(cudaMemsetAsync(*sp[k], 0, S * 8, c->stream));
   }
   double **sz[] = {&c->hydf_surf, &c->abyd_surf, &c->calc_rech, &c->rech_base, &c->sea_hydf, &c->sea_abyd,
-                   &c->drain, &c->surf_head, &c->surf_old};
+                   &c->drain, &c->surf_head, &c->surf_old, &c->top_invd};
   for (auto q : sz) { ALLOC(*q, S * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, S * 8, c->stream)); }
   ALLOC(c->offind, (N + 1) * 4);
   double **vn[] = {&c->head_new, &c->head_old, &c->head_old2, &c->head_pre, &c->head_change, &c->srat_new, &c->srat_old,
@@ -927,6 +927,20 @@ int msg_gpu_cell_mass(msg_ctx_t *c, double *sto, double *con, double *sea, doubl
   return MSG_OK;
 }
 
+int msg_gpu_velocity(msg_ctx_t *c, double *facev, double *pointv) {
+  if (!c) return MSG_ERR_ARG;
+  const size_t N = c->N;
+  double *dv = nullptr;
+  ALLOC(dv, 9 * N * 8);
+  int rc = launch_velocity(c, dv, dv + 6 * N);
+  if (rc) { cudaFree(dv); return rc; }
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  if (facev) MSG_CUDA(cudaMemcpy(facev, dv, 6 * N * 8, cudaMemcpyDeviceToHost));
+  if (pointv) MSG_CUDA(cudaMemcpy(pointv, dv + 6 * N, 3 * N * 8, cudaMemcpyDeviceToHost));
+  cudaFree(dv);
+  return MSG_OK;
+}
+
 int msg_gpu_water_table(msg_ctx_t *c, double *wtable) {
   if (!c || !wtable) return MSG_ERR_ARG;
   int rc = launch_water_table(c, c->tmpv);   // tmpv: N >= S doubles of scratch
@@ -1063,6 +1077,7 @@ static void free_ctx(msg_ctx *c) {
   amg_free(c);
   learned_free(c);
   void *dp[] = {c->reta, c->retn, c->resi, c->poro, c->ss, c->ksz, c->cell_top, c->cell_vol, c->hy, c->ab,
+                c->invd, c->top_invd,
                 c->surf_top, c->surf_bott, c->surf_reli, c->surf_parm, c->hydf_surf, c->abyd_surf, c->calc_rech,
                 c->rech_base, c->sea_hydf, c->sea_abyd, c->read_seal, c->drain, c->offind, c->offrow, c->conn_dir,
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,

@@ -30,6 +30,8 @@ struct msg_ctx {
   float *reta, *retn, *resi, *poro, *ss;        // [N] real(SP)
   double *cell_top, *cell_vol;                   // [N]
   double *hy, *ab;                               // [3N] hydf / abyd of the up, north, west face of each cell
+  double *invd;                                  // [3N] 1/dis12 of the same faces (velocity output)
+  double *top_invd;                              // [S] 1/dis2face(up) of each top cell (surface and sea faces)
   float *ksz;                                    // [N] kept for the drainage and surface coefficients
   // ---- surface (top layer) and boundary arrays [S] -----------------------------------
   double *surf_top, *surf_bott, *surf_reli, *surf_parm, *hydf_surf, *abyd_surf;
@@ -97,6 +99,7 @@ int launch_make_matvec(msg_ctx *c, bool reuse = false);
 // Export the DIA Jacobian into the reference CSR order.
 int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
 int launch_mass(msg_ctx *c, double *out9_dev);
+int launch_velocity(msg_ctx *c, double *facev, double *pointv);
 int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *rec, double *sur,
                      double *drn);
 

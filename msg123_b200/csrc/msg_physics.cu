@@ -45,7 +45,7 @@ __global__ void k_faces(Geo g, int sea_top, int free_drainage, const float *__re
                         const float *__restrict__ ksy, const float *__restrict__ ksz,
                         const double *__restrict__ dis, const double *__restrict__ far,
                         double *hy, double *ab, double *hydf_surf, double *abyd_surf,
-                        double *sea_hydf, double *sea_abyd, double *drain) {
+                        double *sea_hydf, double *sea_abyd, double *drain, double *invd, double *top_invd) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -57,10 +57,13 @@ __global__ void k_faces(Geo g, int sea_top, int free_drainage, const float *__re
     double d1 = dis[0 * N + i], d2 = dis[5 * N + nb];
     hy[0 * N + i] = sat_hyd((double)ksz[i], (double)ksz[nb], d1, d2);
     ab[0 * N + i] = __ddiv_rn(far[0 * N + i], __dadd_rn(d1, d2));
+    invd[0 * N + i] = __ddiv_rn(1.0, __dadd_rn(d1, d2));
   } else {
-    hy[0 * N + i] = 0.0; ab[0 * N + i] = 0.0;
+    hy[0 * N + i] = 0.0; ab[0 * N + i] = 0.0; invd[0 * N + i] = 0.0;
     int s = i;
     double d1 = dis[0 * N + i];
+    // sea face (dis12 = d1) and surface term (surf_elev - cell_cent = d1) share 1/d1
+    top_invd[s] = __ddiv_rn(1.0, d1);
     if (sea_top) {
       sea_hydf[s] = (double)ksz[i];                       // bf == 1: hydf = tks
       sea_abyd[s] = __ddiv_rn(far[0 * N + i], d1);        // dis12 = d1
@@ -78,8 +81,9 @@ __global__ void k_faces(Geo g, int sea_top, int free_drainage, const float *__re
     double d1 = dis[1 * N + i], d2 = dis[4 * N + nb];
     hy[1 * N + i] = sat_hyd((double)ksy[i], (double)ksy[nb], d1, d2);
     ab[1 * N + i] = __ddiv_rn(far[1 * N + i], __dadd_rn(d1, d2));
+    invd[1 * N + i] = __ddiv_rn(1.0, __dadd_rn(d1, d2));
   } else {
-    hy[1 * N + i] = 0.0; ab[1 * N + i] = 0.0;
+    hy[1 * N + i] = 0.0; ab[1 * N + i] = 0.0; invd[1 * N + i] = 0.0;
   }
   // west
   if (ix > 0) {
@@ -87,8 +91,9 @@ __global__ void k_faces(Geo g, int sea_top, int free_drainage, const float *__re
     double d1 = dis[2 * N + i], d2 = dis[3 * N + nb];
     hy[2 * N + i] = sat_hyd((double)ksx[i], (double)ksx[nb], d1, d2);
     ab[2 * N + i] = __ddiv_rn(far[2 * N + i], __dadd_rn(d1, d2));
+    invd[2 * N + i] = __ddiv_rn(1.0, __dadd_rn(d1, d2));
   } else {
-    hy[2 * N + i] = 0.0; ab[2 * N + i] = 0.0;
+    hy[2 * N + i] = 0.0; ab[2 * N + i] = 0.0; invd[2 * N + i] = 0.0;
   }
   if (iz == g.nz - 1) {
     int s = i - (g.nz - 1) * g.nxy;
@@ -501,6 +506,59 @@ __global__ void __launch_bounds__(256) k_cell_mass(FluxArgs a, const double *h_o
   if (i >= (a.g.nz - 1) * a.g.nxy) drn[i - (a.g.nz - 1) * a.g.nxy] = acc[5];
 }
 
+// calc_outvelc (Calc_output.f90:168-241) for cell i: the Darcy velocity through each face
+// (face-major facev[d*N + i], d = up, north, west, east, south, down): regular faces
+// hydf * relat * delhead * (1/dis12) in the reference's product order; the top face the
+// sea term (sea layer above) or else the surface term, both with 1/dis2face(up); the bottom
+// face of the lowest layer the unit-gradient velocity -Ksz kr under free drainage (an
+// extension); faces with no connection 0.  Then the cell-centred components pointv[c*N + i]
+// (c = x, y, z) from the opposite face pairs: half the difference where the two velocities
+// have opposite signs, the whole difference otherwise, z negated (upward positive).
+__global__ void __launch_bounds__(256) k_velocity(FluxArgs a, const double *invd, const double *top_invd,
+                                                  const float *ksz, double *facev, double *pointv) {
+  const Geo g = a.g;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  const size_t N = g.N;
+  int ix, iy, iz;
+  cell_ijk(g, i, ix, iy, iz);
+  const double hi = a.h[i], kri = a.kr[i];
+  const int nbd[6] = {-g.nxy, -g.nx, -1, 1, g.nx, g.nxy};
+  const bool has[6] = {iz > 0, iy > 0, ix > 0, ix < g.nx - 1, iy < g.ny - 1, iz < g.nz - 1};
+  double fv[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    fv[d] = 0.0;
+    if (has[d]) {
+      int j = i + nbd[d];
+      size_t fi = (d < 3) ? (size_t)d * N + i : (size_t)(5 - d) * N + j;
+      double delhead = __dsub_rn(a.h[j], hi);
+      double relat = upwind(-delhead, kri, a.kr[j]);
+      fv[d] = __dmul_rn(__dmul_rn(__dmul_rn(a.hy[fi], relat), delhead), invd[fi]);
+    }
+  }
+  if (iz == 0) {
+    if (a.sea_top) {
+      double delhead = __dsub_rn(a.read_seal[i], hi);
+      fv[0] = __dmul_rn(__dmul_rn(__dmul_rn(a.sea_hydf[i], delhead), top_invd[i]), kri);
+    } else {
+      double delhead = __dsub_rn(a.surf_head[i], hi);
+      fv[0] = __dmul_rn(__dmul_rn(__dmul_rn(a.hydf_surf[i], delhead), top_invd[i]), kri);
+    }
+  }
+  if (a.free_drainage && iz == g.nz - 1) fv[5] = -__dmul_rn((double)ksz[i], kri);
+#pragma unroll
+  for (int d = 0; d < 6; ++d) facev[(size_t)d * N + i] = fv[d];
+#pragma unroll
+  for (int d = 1; d <= 3; ++d) {
+    double x = fv[d - 1], y = fv[6 - d], v;
+    if ((x > 0.0 && y < 0.0) || (x < 0.0 && y > 0.0)) v = __dmul_rn(__dsub_rn(x, y), 0.5);
+    else v = __dsub_rn(x, y);
+    if (d == 1) v = -v;
+    pointv[(size_t)(3 - d) * N + i] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Host wrappers
 // ---------------------------------------------------------------------------------
@@ -522,7 +580,7 @@ int build_connectivity(msg_ctx *c, const msg_grid_t *g) {
   Geo gg = geo(c);
   k_faces<<<nblk(c->N), kThreads, 0, c->stream>>>(gg, c->sea_top, c->free_drainage, d_ksx, d_ksy, c->ksz, d_dis,
                                                      d_far, c->hy, c->ab, c->hydf_surf, c->abyd_surf, c->sea_hydf,
-                                                     c->sea_abyd, c->drain);
+                                                     c->sea_abyd, c->drain, c->invd, c->top_invd);
   MSG_CHECK_LAUNCH();
   // CSR
   int *cnt, *lcnt, *rcnt, *lscan, *rscan;
@@ -689,6 +747,16 @@ int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *
   a.surf_head = c->surf_old;
   k_cell_mass<<<nblk(c->N), 256, 0, c->stream>>>(a, c->head_old, c->srat_old, c->srat_new, c->alp, alp_old, c->poro,
                                                   c->cell_vol, c->delt_inv, c->delt, sto, con, sea, rec, sur, drn);
+  MSG_CHECK_LAUNCH();
+  return MSG_OK;
+}
+
+int launch_velocity(msg_ctx *c, double *facev, double *pointv) {
+  // rel_perm at head_new, as calc_outvelc reads it after the step
+  int rc;
+  if ((rc = launch_srat_rperm(c, c->head_new, 0.0, c->srat_new, c->kr, c->alp))) return rc;
+  FluxArgs a = flux_args(c, c->head_new);
+  k_velocity<<<nblk(c->N), 256, 0, c->stream>>>(a, c->invd, c->top_invd, c->ksz, facev, pointv);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }

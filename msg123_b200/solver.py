@@ -310,6 +310,15 @@ class GpuSolver:
         _check(L.msg_gpu_cell_mass(self.h, *(dptr(out[k]) for k, _ in keys)), "cell_mass")
         return out
 
+    def velocity(self):
+        """calc_outvelc (Calc_output.f90:168-241) at head_new: (facev [6, ncalc] face-major,
+        pointv [3, ncalc] x, y, z)."""
+        L = load_library()
+        L.msg_gpu_velocity.argtypes = [C.c_void_p, abi.PD, abi.PD]
+        fv, pv = np.zeros(6 * self.n), np.zeros(3 * self.n)
+        _check(L.msg_gpu_velocity(self.h, dptr(fv), dptr(pv)), "velocity")
+        return fv.reshape(6, self.n), pv.reshape(3, self.n)
+
     def amg_sizes(self):
         """(rows, off-diagonal entries, prolongation entries from the level above) of each
         level of the last AMG setup, level 0 = Jacobian (its prolongation count is 0)."""

@@ -56,6 +56,7 @@ typedef struct orc {
   int *offind, *offrow, *conn_dir, *left_off, *right_off;
   double *area_dis, *sat_hydf;
   int nseal; int *sea2cal, *sea2sea; double *sea_abyd, *sea_hydf, *read_seal;
+  double *conn_dis, *sea_dis;   /* 1/dis12 per connection and per sea face (velocity output) */
   double *surf_area, *rech_area, *hydf_surf, *abyd_surf, *surf_dis;
   double *surf_top, *surf_bott, *surf_reli, *surf_parm;
   double *calc_rech, *rech_base, *drain_coef;
@@ -107,6 +108,8 @@ static void orc_connect(orc_t *o) {
   o->right_off = xc((size_t)6 * N, sizeof(int));
   o->area_dis = xc((size_t)6 * N, sizeof(double));
   o->sat_hydf = xc((size_t)6 * N, sizeof(double));
+  o->conn_dis = xc((size_t)6 * N, sizeof(double));
+  o->sea_dis = xc((size_t)6 * o->ncals + 1, sizeof(double));
   o->sea2cal = xc((size_t)6 * o->ncals + 1, sizeof(int));
   o->sea2sea = xc((size_t)6 * o->ncals + 1, sizeof(int));
   o->sea_abyd = xc((size_t)6 * o->ncals + 1, sizeof(double));
@@ -138,6 +141,7 @@ static void orc_connect(orc_t *o) {
         sat_hyd(1, tks, 0.0, dis1, dis1, &hyd);
         o->sea_abyd[nseal - 1] = FAR(i, 1) / dis12;
         o->sea_hydf[nseal - 1] = hyd;
+        o->sea_dis[nseal - 1] = DONE / dis12;
       } else {
         int nb = i - nxy;
         double aks = o->ksz[nb];
@@ -147,6 +151,7 @@ static void orc_connect(orc_t *o) {
         dis1 = DIS(i, 1); dis2 = DIS(nb, 6); dis12 = dis1 + dis2;
         sat_hyd(0, tks, aks, dis1, dis2, &hyd);
         o->area_dis[tconn - 1] = FAR(i, 1) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
       }
     } else if (i < o->ncals) {
       o->surf_area[i] = FAR(i, 1);
@@ -162,6 +167,7 @@ static void orc_connect(orc_t *o) {
       dis1 = DIS(i, 2); dis2 = DIS(nb, 5); dis12 = dis1 + dis2;
       sat_hyd(0, tks, aks, dis1, dis2, &hyd);
       o->area_dis[tconn - 1] = FAR(i, 2) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
     }
     /* west */
     if (i_num != 1) {
@@ -172,6 +178,7 @@ static void orc_connect(orc_t *o) {
       dis1 = DIS(i, 3); dis2 = DIS(nb, 4); dis12 = dis1 + dis2;
       sat_hyd(0, tks, aks, dis1, dis2, &hyd);
       o->area_dis[tconn - 1] = FAR(i, 3) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
     }
     /* east */
     if (i_num != nx) {
@@ -182,6 +189,7 @@ static void orc_connect(orc_t *o) {
       dis1 = DIS(i, 4); dis2 = DIS(nb, 3); dis12 = dis1 + dis2;
       sat_hyd(0, tks, aks, dis1, dis2, &hyd);
       o->area_dis[tconn - 1] = FAR(i, 4) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
     }
     /* south */
     if (j_num != ny) {
@@ -192,6 +200,7 @@ static void orc_connect(orc_t *o) {
       dis1 = DIS(i, 5); dis2 = DIS(nb, 2); dis12 = dis1 + dis2;
       sat_hyd(0, tks, aks, dis1, dis2, &hyd);
       o->area_dis[tconn - 1] = FAR(i, 5) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
     }
     /* down */
     if (k_num != o->gridz) {
@@ -202,6 +211,7 @@ static void orc_connect(orc_t *o) {
       dis1 = DIS(i, 6); dis2 = DIS(nb, 1); dis12 = dis1 + dis2;
       sat_hyd(0, tks, aks, dis1, dis2, &hyd);
       o->area_dis[tconn - 1] = FAR(i, 6) / dis12; o->sat_hydf[tconn - 1] = hyd;
+      o->conn_dis[tconn - 1] = DONE / dis12;
     } else if (o->free_drainage) {
       /* free drainage (extension): unit-gradient outflow K*kr*A through the bottom face */
       o->drain_coef[i] = (double)o->ksz[i] * FAR(i, 6);
@@ -1316,6 +1326,52 @@ static void cell_mass(orc_t *o, double *stom, double *conm, double *seam, double
   free(an); free(ao); free(so); free(kr); free(flow);
 }
 
+/* calc_outvelc (Calc_output.f90:168-241): Darcy velocity through each face of each cell,
+ * facev [6][ncalc] face-major (face order up, north, west, east, south, down), and the
+ * cell-centred components pointv [3][ncalc] (x, y, z), at head_new with rel_perm at
+ * head_new.  Faces with no connection stay zero, as in the reference's zeroed output
+ * array.  The surface term's 1/(surf_elev - cell_cent) is 1/dis2face(i,1) bit for bit:
+ * surf_elev = fp_zt and cell_cent = cp_z = (fp_zt + fp_zb)/2 for a top cell, and
+ * dis2face(i,1) = fp_zt - cp_z (Make_cell.f90:119,147,351,358).  Free drainage (an
+ * extension) gives the bottom face of the lowest cells the unit-gradient velocity
+ * -Ksz kr. */
+static void outvelc(orc_t *o, double *facev, double *pointv) {
+  int N = o->ncalc, S = o->ncals;
+  double *sr = xc(N, sizeof(double)), *al = xc(N, sizeof(double));
+  srat_rperm(o, DZERO, o->head_new, sr, o->rel_perm, al);
+  memset(facev, 0, sizeof(double) * 6 * (size_t)N);
+  const double *h = o->head_new, *kr = o->rel_perm;
+  for (int i = 0; i < N; ++i)
+    for (int ind = o->offind[i]; ind < o->offind[i + 1]; ++ind) {
+      int j = o->offrow[ind];
+      double delhead = h[j] - h[i];
+      double relat = hyd_upwind(-delhead, kr[i], kr[j]);
+      int dir = o->conn_dir[ind];
+      facev[(size_t)(dir - 1) * N + i] = o->sat_hydf[ind] * relat * delhead * o->conn_dis[ind];
+    }
+  for (int i = 0; i < S; ++i) {
+    double invdis = DONE / o->dis2face[i];               /* 1/(surf_elev - cell_cent) */
+    double delhead = o->surf_head[i] - h[i];
+    facev[i] = o->hydf_surf[i] * delhead * invdis * kr[i];
+  }
+  for (int k = 0; k < o->nseal; ++k) {
+    int c = o->sea2cal[k], s = o->sea2sea[k];
+    double delhead = o->read_seal[s] - h[c];
+    facev[c] = o->sea_hydf[k] * delhead * o->sea_dis[k] * kr[c];   /* sea faces are up faces */
+  }
+  for (int i = 0; i < N; ++i)
+    if (o->drain_coef[i] != DZERO) facev[(size_t)5 * N + i] = -((double)o->ksz[i] * kr[i]);
+  for (int i = 0; i < N; ++i)
+    for (int d = 1; d <= 3; ++d) {
+      double a = facev[(size_t)(d - 1) * N + i], b = facev[(size_t)(6 - d) * N + i], v;
+      if ((a > DZERO && b < DZERO) || (a < DZERO && b > DZERO)) v = (a - b) * 0.5;
+      else v = a - b;
+      if (d == 1) v = -v;
+      pointv[(size_t)(3 - d) * N + i] = v;
+    }
+  free(sr); free(al);
+}
+
 /* =================================================================================
  * Exported API (ctypes), mirroring include/msg123_gpu.h entry points.
  * =================================================================================*/
@@ -1479,6 +1535,7 @@ int orc_advance(void *h, int nsteps, double rech_until, double rech_after, msg_r
 }
 
 void orc_calc_mass(void *h, double *out9) { calc_mass((orc_t *)h, out9); }
+void orc_velocity(void *h, double *facev, double *pointv) { outvelc((orc_t *)h, facev, pointv); }
 void orc_cell_mass(void *h, double *sto, double *con, double *sea, double *rec, double *sur, double *drn) {
   cell_mass((orc_t *)h, sto, con, sea, rec, sur, drn);
 }

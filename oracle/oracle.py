@@ -49,6 +49,7 @@ def lib():
         L.orc_set_state.argtypes = [vp, abi.PD, abi.PD, abi.PD, abi.PD, C.c_double]
         L.orc_srat_rperm.argtypes = [vp, abi.PD, C.c_double, abi.PD, abi.PD, abi.PD]
         L.orc_cell_mass.argtypes = [vp] + [abi.PD] * 6
+        L.orc_velocity.argtypes = [vp, abi.PD, abi.PD]
         L.orc_amg_level_sizes.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PI]
         L.orc_amg_level.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
         _lib = L
@@ -202,6 +203,13 @@ class Oracle:
                    drn=np.zeros(S))
         lib().orc_cell_mass(C.c_void_p(self.h), *(dptr(out[k]) for k in ("sto", "con", "sea", "rec", "sur", "drn")))
         return out
+
+    def velocity(self):
+        """calc_outvelc: (facev [6, ncalc] face-major, pointv [3, ncalc] x, y, z)."""
+        N = self.prob.ncalc
+        fv, pv = np.zeros(6 * N), np.zeros(3 * N)
+        lib().orc_velocity(C.c_void_p(self.h), dptr(fv), dptr(pv))
+        return fv.reshape(6, N), pv.reshape(3, N)
 
     def counters(self):
         return {k: lib().orc_counter(C.c_void_p(self.h), i) for i, k in enumerate(("func", "matvec", "prec"))}

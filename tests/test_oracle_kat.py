@@ -806,3 +806,29 @@ def test_cell_mass_sums_to_calc_mass(name, kw):
     assert abs(bottom.sum() - tot[8]) <= 1e-13 * max(abs(tot[8]), 1e-300)
     if not p.free_drainage:
         assert not np.any(bottom)
+
+
+def test_velocity_unit_gradient_column():
+    """calc_outvelc on a saturated column under a unit head gradient: every interior face
+    carries the saturated conductivity, inward from above and outward below (facev(up) =
+    +Ks, facev(down) = -Ks), so the cell-centred vertical velocity is -Ks (downward, the
+    half-difference of the opposite-signed pair); the horizontal components are zero and
+    the bottom face of the lowest cell carries the free-drainage velocity -Ks."""
+    p = make_config("box", shape=(1, 1, 6))
+    o = Oracle(p)
+    o.init_state()
+    dz = p.cell_top[0] - p.cell_top[1]
+    h = np.full(p.ncalc, p.cell_top[0] + 0.5)         # equal heads, saturated: no flow between cells
+    o.set_state(head_new=h, head_old=h, srat_old=np.ones(p.ncalc), surf_head=h[:1])
+    fv, pv = o.velocity()
+    assert not np.any(fv[1:5]) and not np.any(fv[0, 1:]) and not np.any(fv[5, :-1])
+    h2 = p.cell_top[0] + 0.5 - dz * np.arange(p.ncalc)   # head drops by dz per cell: unit gradient
+    o.set_state(head_new=h2, head_old=h2, srat_old=np.ones(p.ncalc), surf_head=h2[:1])
+    fv, pv = o.velocity()
+    ks = float(p.ksz[0])
+    inner = np.arange(1, p.ncalc - 1)
+    assert np.allclose(fv[0, inner], ks, rtol=1e-12)
+    assert np.allclose(fv[5, inner], -ks, rtol=1e-12)
+    assert np.allclose(pv[2, inner], -ks, rtol=1e-12)
+    assert not np.any(pv[:2])
+    assert fv[5, -1] == -ks                            # free drainage at the bottom, kr = 1
