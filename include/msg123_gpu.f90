@@ -105,6 +105,20 @@ module msg_gpu
       import; type(c_ptr), value :: ctx; real(c_double), intent(in) :: x(*), v(*)
       real(c_double), intent(out) :: out(*)
     end function
+    integer(c_int) function msg_gpu_set_wells(ctx, nwell, well_index, well_conn, abyd_well, well_bott, read_well) &
+        bind(C)
+      import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: nwell
+      integer(c_int32_t), intent(in) :: well_index(*), well_conn(*)
+      real(c_double), intent(in) :: abyd_well(*), well_bott(*), read_well(*)
+    end function
+    integer(c_int) function msg_gpu_set_rivers(ctx, n, rive2cals, rive_head, rive_bott, abyd_rive) bind(C)
+      import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: n; integer(c_int32_t), intent(in) :: rive2cals(*)
+      real(c_double), intent(in) :: rive_head(*), rive_bott(*), abyd_rive(*)
+    end function
+    integer(c_int) function msg_gpu_set_lakes(ctx, n, lake2cals, lake_head, lake_bott, abyd_lake) bind(C)
+      import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: n; integer(c_int32_t), intent(in) :: lake2cals(*)
+      real(c_double), intent(in) :: lake_head(*), lake_bott(*), abyd_lake(*)
+    end function
     integer(c_int) function msg_gpu_calc_numsol(ctx, st) bind(C)
       import; type(c_ptr), value :: ctx; type(msg_stats_t), intent(out) :: st
     end function

@@ -225,6 +225,30 @@ MSG_API int msg_gpu_calc_numsol(msg_ctx_t *ctx, msg_stats_t *stats);
 MSG_API int msg_gpu_advance(msg_ctx_t *ctx, int32_t nsteps, double rech_until, double rech_after,
                     msg_run_stats_t *stats);
 
+/* Wells, rivers and lakes (the reference's well / river / lake boundary terms).  Each call
+ * replaces the table; n = 0 removes it.  Cells are 1-based as the reference stores them.
+ *
+ * msg_gpu_set_wells: the well connectivity set_wellconn builds -- well_index [nwell+1]
+ * prefix offsets (well_index[0] = 0), well_conn [well_index[nwell]] cells, abyd_well per
+ * connection -- and per well its bottom well_bott and pumping volume rate read_well.  At
+ * the start of every time step after an accepted one (and of the first), msg_gpu_advance
+ * sets the per-cell rates as set_vwell_head does (Time_module.f90:1137-1158 with
+ * calc_vheadout / calc_vheadin, :1253-1335); calc_func adds them as func_wellterm does
+ * (Calc_function.f90:277-302), with no Jacobian entry, as in make_matrix.  A cell may belong
+ * to one well only.
+ *
+ * msg_gpu_set_rivers / msg_gpu_set_lakes: rive2cals / lake2cals (top-layer cells, each at
+ * most once), stage, bed elevation and area/distance abyd_rive / abyd_lake of each river or
+ * lake cell: func_riveterm / func_laketerm (Calc_function.f90:393-473) in the residual and
+ * set_rivebound / set_lakebound (Make_linearsystem.f90:287-408) in the Jacobian diagonal.
+ * Call again whenever the stages change (the reference's time series). */
+MSG_API int msg_gpu_set_wells(msg_ctx_t *ctx, int32_t nwell, const int32_t *well_index, const int32_t *well_conn,
+                              const double *abyd_well, const double *well_bott, const double *read_well);
+MSG_API int msg_gpu_set_rivers(msg_ctx_t *ctx, int32_t n, const int32_t *rive2cals, const double *rive_head,
+                               const double *rive_bott, const double *abyd_rive);
+MSG_API int msg_gpu_set_lakes(msg_ctx_t *ctx, int32_t n, const int32_t *lake2cals, const double *lake_head,
+                              const double *lake_bott, const double *abyd_lake);
+
 /* calc_mass (Calc_function.f90:103-174) summed over cells: out[0..7] =
  * storage, flow, recharge, well, surface, river, lake, sea (+ out[8] drainage),
  * each a volume over the step (rate * delt). */
@@ -235,8 +259,7 @@ MSG_API int msg_gpu_calc_mass(msg_ctx_t *ctx, double *out9);
  * neighbours, sea-face inflow, wells); rec, sur, riv, lak: [ncals] (recharge, surface,
  * river, lake); drn: [ncals] outflow through the bottom face of each column under free
  * drainage (extension, no reference column).  Each a rate times delt, summing to the
- * msg_gpu_calc_mass totals.  No wells, rivers or lakes are modelled, so wel, riv and lak
- * come back zero.  Any pointer may be NULL. */
+ * msg_gpu_calc_mass totals.  Any pointer may be NULL. */
 MSG_API int msg_gpu_cell_mass(msg_ctx_t *ctx, double *sto, double *con, double *sea, double *wel, double *rec,
                               double *sur, double *riv, double *lak, double *drn);
 /* calc_outvelc (Calc_output.f90:168-241) at the current head_new (relative permeability

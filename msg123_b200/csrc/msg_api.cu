@@ -449,6 +449,10 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
     MSG_CHECK_LAUNCH();
     c->current_t = (double)(float)(c->current_t + (double)(float)c->delt);
     c->delt_inv = 1.0 / c->delt;
+    // update_tstep (Time_module.f90:83-87): well rates after an accepted step or at the start
+    if ((conv == 1 || c->timestep_num == 0) && c->nwell > 0) {
+      if ((rc = launch_wells(c))) return rc;
+    }
     msg_stats_t st;
     bool learned_try = false;
     if (c->prm.guess_mode == 2 && c->timestep_num > 0 && conv != 0 && learned_ready(c)) {
@@ -684,6 +688,11 @@ int msg_gpu_copy_state(msg_ctx_t *dst, const msg_ctx_t *src) {
   dst->delt = src->delt; dst->delt_inv = src->delt_inv;
   dst->delt_old1 = src->delt_old1; dst->delt_old2 = src->delt_old2;
   dst->timestep_num = src->timestep_num; dst->last_conv = src->last_conv; dst->last_out = src->last_out;
+  // dst's own well table applied to the copied head (as at the start of the step)
+  if (dst->nwell > 0) {
+    int rc = launch_wells(dst);
+    if (rc) return rc;
+  }
   MSG_CUDA(cudaStreamSynchronize(dst->stream));
   return MSG_OK;
 }
@@ -910,20 +919,22 @@ int msg_gpu_cell_mass(msg_ctx_t *c, double *sto, double *con, double *sea, doubl
                       double *riv, double *lak, double *drn) {
   if (!c) return MSG_ERR_ARG;
   const size_t N = c->N, S = c->S;
-  // Krylov scratch vectors (free between solves) hold the device copies
-  int rc = launch_cell_mass(c, c->r, c->rs, c->v, c->p, c->t, c->z);
-  if (rc) return rc;
+  // Krylov scratch vectors (free between solves) hold the device copies: r, rs, v, p get
+  // the [N] arrays; t holds the five [S] arrays back to back (N >= 5S needs nz >= 5, else
+  // a temporary)
+  double *ts = c->t;
+  if ((size_t)N < 5 * S) ALLOC(ts, 5 * S * 8);
+  int rc = launch_cell_mass(c, c->r, c->rs, c->v, c->p, ts, ts + S, ts + 2 * S, ts + 3 * S, ts + 4 * S);
+  if (rc) { if (ts != c->t) cudaFree(ts); return rc; }
   MSG_CUDA(cudaStreamSynchronize(c->stream));
   if (sto) MSG_CUDA(cudaMemcpy(sto, c->r, N * 8, cudaMemcpyDeviceToHost));
   if (con) MSG_CUDA(cudaMemcpy(con, c->rs, N * 8, cudaMemcpyDeviceToHost));
   if (sea) MSG_CUDA(cudaMemcpy(sea, c->v, N * 8, cudaMemcpyDeviceToHost));
-  if (rec) MSG_CUDA(cudaMemcpy(rec, c->p, S * 8, cudaMemcpyDeviceToHost));
-  if (sur) MSG_CUDA(cudaMemcpy(sur, c->t, S * 8, cudaMemcpyDeviceToHost));
-  if (drn) MSG_CUDA(cudaMemcpy(drn, c->z, S * 8, cudaMemcpyDeviceToHost));
-  // no wells, rivers or lakes exist in a context: their volumes are zero
-  if (wel) memset(wel, 0, N * 8);
-  if (riv) memset(riv, 0, S * 8);
-  if (lak) memset(lak, 0, S * 8);
+  if (wel) MSG_CUDA(cudaMemcpy(wel, c->p, N * 8, cudaMemcpyDeviceToHost));
+  double *hs[5] = {rec, sur, riv, lak, drn};
+  for (int q = 0; q < 5; ++q)
+    if (hs[q]) MSG_CUDA(cudaMemcpy(hs[q], ts + q * S, S * 8, cudaMemcpyDeviceToHost));
+  if (ts != c->t) cudaFree(ts);
   return MSG_OK;
 }
 
@@ -939,6 +950,91 @@ int msg_gpu_velocity(msg_ctx_t *c, double *facev, double *pointv) {
   if (pointv) MSG_CUDA(cudaMemcpy(pointv, dv + 6 * N, 3 * N * 8, cudaMemcpyDeviceToHost));
   cudaFree(dv);
   return MSG_OK;
+}
+
+int msg_gpu_set_wells(msg_ctx_t *c, int32_t nwell, const int32_t *well_index, const int32_t *well_conn,
+                      const double *abyd_well, const double *well_bott, const double *read_well) {
+  if (!c || nwell < 0) { set_error("set_wells: bad arguments"); return MSG_ERR_ARG; }
+  int *wi = c->w_index, *wc = c->w_conn;
+  double *wa = c->w_abyd, *wb = c->w_bott, *wr = c->w_rate;
+  c->w_index = c->w_conn = nullptr; c->w_abyd = c->w_bott = c->w_rate = nullptr;
+  c->nwell = 0;
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(wi); cudaFree(wc); cudaFree(wa); cudaFree(wb); cudaFree(wr);
+  if (nwell == 0) {
+    if (c->calc_well) MSG_CUDA(cudaMemsetAsync(c->calc_well, 0, (size_t)c->N * 8, c->stream));
+    return MSG_OK;
+  }
+  if (!well_index || !well_conn || !abyd_well || !well_bott || !read_well) {
+    set_error("set_wells: NULL array"); return MSG_ERR_ARG;
+  }
+  if (well_index[0] != 0) { set_error("set_wells: well_index[0] must be 0"); return MSG_ERR_ARG; }
+  for (int w = 0; w < nwell; ++w)
+    if (well_index[w + 1] < well_index[w]) { set_error("set_wells: well_index decreases at well %d", w + 1); return MSG_ERR_ARG; }
+  const int nc = well_index[nwell];
+  // a cell may belong to one well only (the reference accumulates calc_well from concurrent
+  // threads, one per well); repeats within one well are added in order
+  std::vector<int> owner(c->N, -1), conn0(nc);
+  for (int w = 0; w < nwell; ++w)
+    for (int k = well_index[w]; k < well_index[w + 1]; ++k) {
+      int j = well_conn[k] - 1;
+      if (j < 0 || j >= c->N) { set_error("set_wells: cell %d of well %d outside 1..%d", j + 1, w + 1, c->N); return MSG_ERR_ARG; }
+      if (owner[j] >= 0 && owner[j] != w) {
+        set_error("set_wells: cell %d belongs to wells %d and %d", j + 1, owner[j] + 1, w + 1); return MSG_ERR_ARG;
+      }
+      owner[j] = w;
+      conn0[k] = j;
+    }
+  ALLOC(c->w_index, (size_t)(nwell + 1) * 4); ALLOC(c->w_conn, (size_t)std::max(nc, 1) * 4);
+  ALLOC(c->w_abyd, (size_t)std::max(nc, 1) * 8); ALLOC(c->w_bott, (size_t)nwell * 8); ALLOC(c->w_rate, (size_t)nwell * 8);
+  if (!c->calc_well) { ALLOC(c->calc_well, (size_t)c->N * 8); }
+  MSG_CUDA(cudaMemsetAsync(c->calc_well, 0, (size_t)c->N * 8, c->stream));
+  UPLOAD(c->w_index, well_index, (size_t)(nwell + 1) * 4);
+  if (nc > 0) { UPLOAD(c->w_conn, conn0.data(), (size_t)nc * 4); UPLOAD(c->w_abyd, abyd_well, (size_t)nc * 8); }
+  UPLOAD(c->w_bott, well_bott, (size_t)nwell * 8);
+  UPLOAD(c->w_rate, read_well, (size_t)nwell * 8);
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  c->nwell = nwell;
+  return MSG_OK;
+}
+
+// Dense [3S] stage / bed / area-by-distance table of the surface cells that carry a river
+// (or lake); zeros elsewhere, which make the terms exact zeros.
+static int set_stage(msg_ctx *c, double **dst, const char *what, int32_t n, const int32_t *cells, const double *head,
+                     const double *bott, const double *abyd) {
+  if (n < 0) { set_error("set_%s: n < 0", what); return MSG_ERR_ARG; }
+  if (n == 0) {
+    MSG_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(*dst); *dst = nullptr;
+    return MSG_OK;
+  }
+  if (!cells || !head || !bott || !abyd) { set_error("set_%s: NULL array", what); return MSG_ERR_ARG; }
+  const int S = c->S;
+  std::vector<double> t((size_t)3 * S, 0.0);
+  std::vector<char> seen(S, 0);
+  for (int k = 0; k < n; ++k) {
+    int s = cells[k] - 1;
+    if (s < 0 || s >= S) { set_error("set_%s: surface cell %d outside 1..%d", what, s + 1, S); return MSG_ERR_ARG; }
+    if (seen[s]) { set_error("set_%s: surface cell %d listed twice", what, s + 1); return MSG_ERR_ARG; }
+    seen[s] = 1;
+    t[s] = head[k]; t[(size_t)S + s] = bott[k]; t[(size_t)2 * S + s] = abyd[k];
+  }
+  if (!*dst) ALLOC(*dst, (size_t)3 * S * 8);
+  UPLOAD(*dst, t.data(), (size_t)3 * S * 8);
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  return MSG_OK;
+}
+
+int msg_gpu_set_rivers(msg_ctx_t *c, int32_t n, const int32_t *rive2cals, const double *rive_head,
+                       const double *rive_bott, const double *abyd_rive) {
+  if (!c) return MSG_ERR_ARG;
+  return set_stage(c, &c->riv, "rivers", n, rive2cals, rive_head, rive_bott, abyd_rive);
+}
+
+int msg_gpu_set_lakes(msg_ctx_t *c, int32_t n, const int32_t *lake2cals, const double *lake_head,
+                      const double *lake_bott, const double *abyd_lake) {
+  if (!c) return MSG_ERR_ARG;
+  return set_stage(c, &c->lak, "lakes", n, lake2cals, lake_head, lake_bott, abyd_lake);
 }
 
 int msg_gpu_water_table(msg_ctx_t *c, double *wtable) {
@@ -1077,7 +1173,8 @@ static void free_ctx(msg_ctx *c) {
   amg_free(c);
   learned_free(c);
   void *dp[] = {c->reta, c->retn, c->resi, c->poro, c->ss, c->ksz, c->cell_top, c->cell_vol, c->hy, c->ab,
-                c->invd, c->top_invd,
+                c->invd, c->top_invd, c->w_index, c->w_conn, c->w_abyd, c->w_bott, c->w_rate, c->calc_well,
+                c->riv, c->lak,
                 c->surf_top, c->surf_bott, c->surf_reli, c->surf_parm, c->hydf_surf, c->abyd_surf, c->calc_rech,
                 c->rech_base, c->sea_hydf, c->sea_abyd, c->read_seal, c->drain, c->offind, c->offrow, c->conn_dir,
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,

@@ -38,6 +38,12 @@ struct msg_ctx {
   double *calc_rech, *rech_base;
   double *sea_hydf, *sea_abyd, *read_seal;
   double *drain;                                 // [S] bottom-layer drainage coefficient
+  // ---- wells, rivers, lakes (msg_gpu_set_wells / _rivers / _lakes; null when none) -----
+  int nwell;
+  int *w_index, *w_conn;                         // [nwell+1] prefix offsets, [nconn] 0-based cells
+  double *w_abyd, *w_bott, *w_rate;              // per connection / per well / per well
+  double *calc_well;                             // [N] well rates of the time step
+  double *riv, *lak;                             // [3S] stage, bed, area/distance per surface cell
   // ---- reference CSR built on the GPU (export / tests) -------------------------------
   int *offind, *offrow, *conn_dir, *left_off, *right_off;
   double *hydf_conn, *abyd_conn;
@@ -100,8 +106,9 @@ int launch_make_matvec(msg_ctx *c, bool reuse = false);
 int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
 int launch_mass(msg_ctx *c, double *out9_dev);
 int launch_velocity(msg_ctx *c, double *facev, double *pointv);
-int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *rec, double *sur,
-                     double *drn);
+int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
+                     double *riv, double *lak, double *drn);
+int launch_wells(msg_ctx *c);
 
 // ---- msg_linear.cu ----------------------------------------------------------------------------
 int build_wavefront(msg_ctx *c);

@@ -265,6 +265,8 @@ struct FluxArgs {
   const double *h, *kr, *kr_per, *sto, *stod, *hy, *ab;
   const double *surf_top, *surf_bott, *surf_reli, *surf_parm, *hydf_surf, *abyd_surf, *surf_head;
   const double *calc_rech, *sea_hydf, *sea_abyd, *read_seal, *drain;
+  const double *riv, *lak;    // [3S] stage, bed, area/distance per surface cell (nullable: none)
+  const double *calc_well;    // [N] well rates of the time step (nullable: no wells)
   double newper, newper_inv;
   double *F;          // residual (calc_func) or rhs = -F (make_matvec)
   double *dmat, *lu;  // assembly outputs
@@ -303,6 +305,27 @@ __device__ __forceinline__ double surf_term(double infs, double insh, double top
   delh_out = delh;
   over_out = over;
   return __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(hydf, abyd), delh), kri), rati);
+}
+
+// func_riveterm / func_laketerm (Calc_function.f90:393-473) for one surface cell s with
+// stage/bed/abyd in st[s], st[S + s], st[2S + s] (abyd 0 where the cell has none, which
+// makes both the term and its derivative an exact zero), and, for the assembly,
+// set_rivebound / set_lakebound (Make_linearsystem.f90:287-408): -tran kr plus the chord of
+// kr over newper times the head difference while the head is at or above the bed.
+__device__ __forceinline__ double stage_term(const double *st, int S, int s, double infs, double hydf, double kri,
+                                             double krpi, double newper_inv, bool asm_, double &dmat_out) {
+  const double head = st[s], bott = st[S + s], abyd = st[2 * S + s];
+  double delh, over;
+  if (infs >= bott) { delh = __dsub_rn(head, infs); over = 1.0; }
+  else if (head > bott) { delh = __dsub_rn(head, bott); over = 0.0; }
+  else { delh = 0.0; over = 1.0; }
+  if (asm_) {
+    double tran = __dmul_rn(hydf, abyd);
+    double deri = __dmul_rn(-tran, kri);
+    double deri_ks = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dsub_rn(krpi, kri), newper_inv), delh), tran), over);
+    dmat_out = __dadd_rn(deri, deri_ks);
+  }
+  return __dmul_rn(__dmul_rn(__dmul_rn(hydf, abyd), delh), kri);
 }
 
 template <bool ASM>
@@ -358,12 +381,16 @@ __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
       double delh, over;
       double sf = surf_term(hi, a.surf_head[s], a.surf_top[s], a.surf_bott[s], a.surf_reli[s], a.surf_parm[s],
                             a.hydf_surf[s], a.abyd_surf[s], kri, delh, over);
-      fs = __dadd_rn(a.calc_rech[s], sf);
+      // funcvs = recf + surf + rivf + lakf (Calc_function.f90:86-90); dmats = surd + rivd + lakd
+      double rv = 0.0, lk = 0.0, rvd = 0.0, lkd = 0.0;
+      if (a.riv) rv = stage_term(a.riv, g.nxy, s, hi, a.hydf_surf[s], kri, krpi, a.newper_inv, ASM, rvd);
+      if (a.lak) lk = stage_term(a.lak, g.nxy, s, hi, a.hydf_surf[s], kri, krpi, a.newper_inv, ASM, lkd);
+      fs = __dadd_rn(__dadd_rn(__dadd_rn(a.calc_rech[s], sf), rv), lk);
       if (ASM) {
         double tran = __dmul_rn(a.hydf_surf[s], a.abyd_surf[s]);
         double deri_s = __dmul_rn(-tran, kri);
         double deri_ks = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dsub_rn(krpi, kri), a.newper_inv), delh), tran), over);
-        ds = __dadd_rn(deri_s, deri_ks);
+        ds = __dadd_rn(__dadd_rn(__dadd_rn(deri_s, deri_ks), rvd), lkd);
       }
       if (a.sea_top) {
         double delhs = __dsub_rn(a.read_seal[s], hi);
@@ -377,7 +404,9 @@ __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
         }
       }
     }
-    double f = __dadd_rn(__dadd_rn(__dadd_rn(fs, a.sto[i]), cf), sea);
+    // funcv = funcvs + stof + conf + welf + seaf (Calc_function.f90:92-96)
+    const double wel = a.calc_well ? a.calc_well[i] : 0.0;
+    double f = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(fs, a.sto[i]), cf), wel), sea);
     double dd = 0.0;
     if (ASM) dd = __dadd_rn(__dadd_rn(__dadd_rn(ds, a.stod[i]), dc), sead);
     if (a.free_drainage && iz == g.nz - 1) {
@@ -430,14 +459,15 @@ __global__ void k_dia_to_csr(Geo g, const int *offind, const double *lu, double 
 // calc_mass (Calc_function.f90:103-174) terms of cell i, each times delt: acc[0] storage
 // (func_stochn), acc[1] flow from the neighbours in CSR face order (func_connflow),
 // acc[2] recharge (func_rechterm), acc[3] surface (func_surfterm with surf_old), acc[4] sea
-// (func_sealterm: one sea face per top cell), acc[5] free drainage (extension).  acc[2..4]
-// belong to top cells, acc[5] to bottom cells; the others are zero.
+// (func_sealterm: one sea face per top cell), acc[5] free drainage (extension), acc[6] wells
+// (func_wellterm), acc[7] rivers, acc[8] lakes.  acc[2..4], acc[7], acc[8] belong to top
+// cells, acc[5] to bottom cells; the others are zero.
 __device__ __forceinline__ void mass_terms(const FluxArgs &a, int i, const double *h_old, const double *s_old,
                                            const double *s_new, const double *alp_new, const double *alp_old,
                                            const float *poro, const double *vol, double delt_inv, double delt,
-                                           double acc[6]) {
+                                           double acc[9]) {
   const Geo g = a.g;
-  for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+  for (int q = 0; q < 9; ++q) acc[q] = 0.0;
   int ix, iy, iz;
   cell_ijk(g, i, ix, iy, iz);
   double hi = a.h[i], kri = a.kr[i];
@@ -457,12 +487,15 @@ __device__ __forceinline__ void mass_terms(const FluxArgs &a, int i, const doubl
     cf = __dadd_rn(cf, __dmul_rn(__dmul_rn(__dmul_rn(a.hy[fi], relat), a.ab[fi]), delhead));
   }
   acc[1] = __dmul_rn(cf, delt);
+  if (a.calc_well) acc[6] = __dmul_rn(a.calc_well[i], delt);
   if (iz == 0) {
-    double delh, over;
+    double delh, over, dummy;
     double sf = surf_term(hi, a.surf_head[i], a.surf_top[i], a.surf_bott[i], a.surf_reli[i], a.surf_parm[i],
                           a.hydf_surf[i], a.abyd_surf[i], kri, delh, over);
     acc[2] = __dmul_rn(a.calc_rech[i], delt);
     acc[3] = __dmul_rn(sf, delt);
+    if (a.riv) acc[7] = __dmul_rn(stage_term(a.riv, g.nxy, i, hi, a.hydf_surf[i], kri, 0.0, 0.0, false, dummy), delt);
+    if (a.lak) acc[8] = __dmul_rn(stage_term(a.lak, g.nxy, i, hi, a.hydf_surf[i], kri, 0.0, 0.0, false, dummy), delt);
     if (a.sea_top)
       acc[4] = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(a.sea_hydf[i], kri), a.sea_abyd[i]), __dsub_rn(a.read_seal[i], hi)), delt);
   }
@@ -479,30 +512,32 @@ __global__ void __launch_bounds__(256) k_mass(FluxArgs a, const double *h_old, c
                                               double *part9) {
   __shared__ double sh[8];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (i < a.g.N) mass_terms(a, i, h_old, s_old, s_new, alp_new, alp_old, poro, vol, delt_inv, delt, acc);
-  for (int q = 0; q < 6; ++q) {
+  for (int q = 0; q < 9; ++q) {
     double s = block_sum<256>(acc[q], sh);
     if (threadIdx.x == 0) part9[(size_t)q * gridDim.x + blockIdx.x] = s;
   }
 }
 
 // calc_cell_mas (Calc_output.f90:54-91): the same terms per cell, in the reference's
-// arrays -- storage, flow and sea per cell [N]; recharge, surface and drainage per
-// surface column [S] (drainage leaves through the column's bottom cell).
+// arrays -- storage, flow, sea and wells per cell [N]; recharge, surface, river, lake and
+// drainage per surface column [S] (drainage leaves through the column's bottom cell).
 __global__ void __launch_bounds__(256) k_cell_mass(FluxArgs a, const double *h_old, const double *s_old,
                                                    const double *s_new, const double *alp_new,
                                                    const double *alp_old, const float *poro, const double *vol,
                                                    double delt_inv, double delt, double *sto, double *con,
-                                                   double *sea, double *rec, double *sur, double *drn) {
+                                                   double *sea, double *wel, double *rec, double *sur, double *riv,
+                                                   double *lak, double *drn) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.g.N) return;
-  double acc[6];
+  double acc[9];
   mass_terms(a, i, h_old, s_old, s_new, alp_new, alp_old, poro, vol, delt_inv, delt, acc);
   sto[i] = acc[0];
   con[i] = acc[1];
   sea[i] = acc[4];
-  if (i < a.g.nxy) { rec[i] = acc[2]; sur[i] = acc[3]; }
+  wel[i] = acc[6];
+  if (i < a.g.nxy) { rec[i] = acc[2]; sur[i] = acc[3]; riv[i] = acc[7]; lak[i] = acc[8]; }
   if (i >= (a.g.nz - 1) * a.g.nxy) drn[i - (a.g.nz - 1) * a.g.nxy] = acc[5];
 }
 
@@ -556,6 +591,37 @@ __global__ void __launch_bounds__(256) k_velocity(FluxArgs a, const double *invd
     else v = __dsub_rn(x, y);
     if (d == 1) v = -v;
     pointv[(size_t)(3 - d) * N + i] = v;
+  }
+}
+
+// set_vwell_head (Time_module.f90:1137-1158: calc_vheadout / calc_vheadin, :1253-1335), one
+// thread per well, connections in the reference's order: the head without pumping is the
+// kr*abyd-weighted mean of the well's cell heads, the pumping rate over the total
+// conductance raises it, and each cell where that head or the cell's own head is above
+// the well bottom gets kr*abyd*(whead - head) (calc_well zeroed beforehand; a cell belongs
+// to one well).  kr is evaluated at head_new, the state the reference's rel_perm holds there.
+template <int FORM>
+__global__ void k_wells(int nwell, const int *__restrict__ w_index, const int *__restrict__ w_conn,
+                        const double *__restrict__ w_abyd, const double *__restrict__ w_bott,
+                        const double *__restrict__ w_rate, CellArgs a, double *calc_well) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwell) return;
+  double tot_cond = 0.0, tot_flux = 0.0, whead = 0.0;
+  for (int k = w_index[w]; k < w_index[w + 1]; ++k) {
+    int j = w_conn[k];
+    double kr = vg_eval<FORM>(a.h[j], a.top[j], 0.0, a.reta[j], a.retn[j], a.resi[j], a.poro[j], a.ss[j]).kr;
+    tot_cond = __dadd_rn(tot_cond, __dmul_rn(kr, w_abyd[k]));
+    tot_flux = __dadd_rn(tot_flux, __dmul_rn(__dmul_rn(kr, w_abyd[k]), a.h[j]));
+  }
+  if (tot_cond == 0.0) return;
+  whead = __ddiv_rn(tot_flux, tot_cond);
+  whead = __dadd_rn(whead, __ddiv_rn(w_rate[w], tot_cond));
+  for (int k = w_index[w]; k < w_index[w + 1]; ++k) {
+    int j = w_conn[k];
+    if (whead > w_bott[w] || a.h[j] > w_bott[w]) {
+      double kr = vg_eval<FORM>(a.h[j], a.top[j], 0.0, a.reta[j], a.retn[j], a.resi[j], a.poro[j], a.ss[j]).kr;
+      calc_well[j] = __dadd_rn(calc_well[j], __dmul_rn(__dmul_rn(kr, w_abyd[k]), __dsub_rn(whead, a.h[j])));
+    }
   }
 }
 
@@ -654,6 +720,7 @@ static FluxArgs flux_args(msg_ctx *c, const double *h) {
   a.hydf_surf = c->hydf_surf; a.abyd_surf = c->abyd_surf; a.surf_head = c->surf_head;
   a.calc_rech = c->calc_rech; a.sea_hydf = c->sea_hydf; a.sea_abyd = c->sea_abyd; a.read_seal = c->read_seal;
   a.drain = c->drain;
+  a.riv = c->riv; a.lak = c->lak; a.calc_well = c->calc_well;
   a.newper = c->newper; a.newper_inv = c->newper_inv;
   a.F = nullptr; a.dmat = nullptr; a.lu = nullptr; a.part = nullptr;
   a.dmat_f = nullptr; a.lu_f = nullptr;
@@ -716,17 +783,17 @@ int launch_mass(msg_ctx *c, double *out9_dev) {
   a.surf_head = c->surf_old;
   int nb = nblk(c->N);
   double *part9 = nullptr;
-  MSG_CUDA(cudaMalloc(&part9, (size_t)6 * nb * 8));
+  MSG_CUDA(cudaMalloc(&part9, (size_t)9 * nb * 8));
   k_mass<<<nb, 256, 0, c->stream>>>(a, c->head_old, c->srat_old, c->srat_new, c->alp, alp_old, c->poro, c->cell_vol,
                                      c->delt_inv, c->delt, part9);
   MSG_CHECK_LAUNCH();
-  std::vector<double> hp((size_t)6 * nb);
+  std::vector<double> hp((size_t)9 * nb);
   MSG_CUDA(cudaMemcpyAsync(hp.data(), part9, hp.size() * 8, cudaMemcpyDeviceToHost, c->stream));
   MSG_CUDA(cudaStreamSynchronize(c->stream));
   cudaFree(part9);
   double out[9] = {0};
-  const int map[6] = {0, 1, 2, 4, 7, 8};
-  for (int q = 0; q < 6; ++q) {
+  const int map[9] = {0, 1, 2, 4, 7, 8, 3, 5, 6};
+  for (int q = 0; q < 9; ++q) {
     double s = 0.0;
     for (int b = 0; b < nb; ++b) s += hp[(size_t)q * nb + b];
     out[map[q]] = s;
@@ -736,7 +803,8 @@ int launch_mass(msg_ctx *c, double *out9_dev) {
   return MSG_OK;
 }
 
-int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *rec, double *sur, double *drn) {
+int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
+                     double *riv, double *lak, double *drn) {
   // old-level vG (alp_old) into tmpv / kr_per scratch, then new-level into srat_new / kr / alp,
   // as launch_mass does
   double *alp_old = c->tmpv, *s_tmp = c->sto, *kr_tmp = c->kr_per;
@@ -746,7 +814,8 @@ int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *
   FluxArgs a = flux_args(c, c->head_new);
   a.surf_head = c->surf_old;
   k_cell_mass<<<nblk(c->N), 256, 0, c->stream>>>(a, c->head_old, c->srat_old, c->srat_new, c->alp, alp_old, c->poro,
-                                                  c->cell_vol, c->delt_inv, c->delt, sto, con, sea, rec, sur, drn);
+                                                  c->cell_vol, c->delt_inv, c->delt, sto, con, sea, wel, rec, sur,
+                                                  riv, lak, drn);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -757,6 +826,20 @@ int launch_velocity(msg_ctx *c, double *facev, double *pointv) {
   if ((rc = launch_srat_rperm(c, c->head_new, 0.0, c->srat_new, c->kr, c->alp))) return rc;
   FluxArgs a = flux_args(c, c->head_new);
   k_velocity<<<nblk(c->N), 256, 0, c->stream>>>(a, c->invd, c->top_invd, c->ksz, facev, pointv);
+  MSG_CHECK_LAUNCH();
+  return MSG_OK;
+}
+
+int launch_wells(msg_ctx *c) {
+  if (!c->calc_well) return MSG_OK;
+  MSG_CUDA(cudaMemsetAsync(c->calc_well, 0, (size_t)c->N * 8, c->stream));
+  if (c->nwell <= 0) return MSG_OK;
+  CellArgs a = cell_args(c, c->head_new);
+  int nb = (c->nwell + 127) / 128;
+  if (c->prm.vg_form) k_wells<1><<<nb, 128, 0, c->stream>>>(c->nwell, c->w_index, c->w_conn, c->w_abyd, c->w_bott,
+                                                           c->w_rate, a, c->calc_well);
+  else k_wells<0><<<nb, 128, 0, c->stream>>>(c->nwell, c->w_index, c->w_conn, c->w_abyd, c->w_bott, c->w_rate, a,
+                                             c->calc_well);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }

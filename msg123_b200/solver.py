@@ -235,6 +235,30 @@ class GpuSolver:
         L.msg_gpu_write_restart.argtypes = [C.c_void_p, C.c_char_p]
         _check(L.msg_gpu_write_restart(self.h, os.fsencode(path)), "write_restart")
 
+    def set_wells(self, well_index, well_conn, abyd, bott, rate):
+        """Well table (msg_gpu_set_wells): well_index [nwell+1] prefix offsets, well_conn
+        1-based cells, abyd_well per connection; well_bott and pumping rate per well."""
+        L = load_library()
+        L.msg_gpu_set_wells.argtypes = [C.c_void_p, C.c_int32, abi.PI, abi.PI, abi.PD, abi.PD, abi.PD]
+        wi = np.ascontiguousarray(well_index, dtype=np.int32)
+        arrs = (np.ascontiguousarray(well_conn, np.int32), _f64(abyd), _f64(bott), _f64(rate))
+        _check(L.msg_gpu_set_wells(self.h, len(wi) - 1, iptr(wi), iptr(arrs[0]), dptr(arrs[1]), dptr(arrs[2]),
+                                   dptr(arrs[3])), "set_wells")
+
+    def set_rivers(self, cells, head, bott, abyd):
+        """River cells (msg_gpu_set_rivers): 1-based surface cells, stage, bed, area/distance."""
+        self._stage("msg_gpu_set_rivers", cells, head, bott, abyd)
+
+    def set_lakes(self, cells, head, bott, abyd):
+        """Lake cells (msg_gpu_set_lakes): 1-based surface cells, stage, bed, area/distance."""
+        self._stage("msg_gpu_set_lakes", cells, head, bott, abyd)
+
+    def _stage(self, name, cells, head, bott, abyd):
+        fn = getattr(load_library(), name)
+        fn.argtypes = [C.c_void_p, C.c_int32, abi.PI, abi.PD, abi.PD, abi.PD]
+        c = np.ascontiguousarray(cells, dtype=np.int32)
+        _check(fn(self.h, len(c), iptr(c), dptr(_f64(head)), dptr(_f64(bott)), dptr(_f64(abyd))), name)
+
     def set_recharge(self, rech):
         _check(load_library().msg_gpu_set_recharge(self.h, dptr(_f64(rech))), "set_recharge")
 

@@ -57,6 +57,12 @@ typedef struct orc {
   double *area_dis, *sat_hydf;
   int nseal; int *sea2cal, *sea2sea; double *sea_abyd, *sea_hydf, *read_seal;
   double *conn_dis, *sea_dis;   /* 1/dis12 per connection and per sea face (velocity output) */
+  /* wells (set_wellconn's well_index / well_conn / abyd_well, read_well, well_bott) and the
+     per-cell rate calc_well set by set_vwell_head once per accepted step */
+  int nwell; int *w_index, *w_conn; double *w_abyd, *w_bott, *w_rate, *calc_well;
+  /* rivers and lakes: surface cell (rive2cals / lake2cals, 0-based), stage, bottom, area/distance */
+  int nriv; int *riv_cell; double *riv_head, *riv_bott, *riv_abyd;
+  int nlak; int *lak_cell; double *lak_head, *lak_bott, *lak_abyd;
   double *surf_area, *rech_area, *hydf_surf, *abyd_surf, *surf_dis;
   double *surf_top, *surf_bott, *surf_reli, *surf_parm;
   double *calc_rech, *rech_base, *drain_coef;
@@ -316,6 +322,78 @@ static void func_surfterm(orc_t *o, const double *infsurf, const double *inshead
   }
 }
 
+/* func_riveterm / func_laketerm (Calc_function.f90:393-473): exchange with a river or lake
+ * stage through the top cell, upstream of the bed: stage minus head while the head is at
+ * or above the bed, stage minus bed while only the stage is, none otherwise.  out[s] for the
+ * surface cells that carry one; the others keep out's zero. */
+static void stage_term(orc_t *o, int n, const int *cell, const double *head, const double *bott,
+                       const double *abyd, const double *infx, double *out) {
+  for (int i = 0; i < n; ++i) {
+    int s = cell[i];
+    double delh;
+    if (infx[s] >= bott[i]) delh = head[i] - infx[s];
+    else if (head[i] > bott[i]) delh = head[i] - bott[i];
+    else delh = DZERO;
+    out[s] = o->hydf_surf[s] * abyd[i] * delh * o->rel_perm[s];
+  }
+}
+static void func_riveterm(orc_t *o, const double *infx, double *rivf) {
+  stage_term(o, o->nriv, o->riv_cell, o->riv_head, o->riv_bott, o->riv_abyd, infx, rivf);
+}
+static void func_laketerm(orc_t *o, const double *infx, double *lakf) {
+  stage_term(o, o->nlak, o->lak_cell, o->lak_head, o->lak_bott, o->lak_abyd, infx, lakf);
+}
+
+/* set_rivebound / set_lakebound (Make_linearsystem.f90:287-408), form_switch == 1: the
+ * diagonal entry of a river or lake cell, -tran kr plus the chord of kr over newper times
+ * the head difference while the head is at or above the bed (over = 1). */
+static void stage_bound(orc_t *o, int n, const int *cell, const double *head, const double *bott,
+                        const double *abyd, double *dmat_out) {
+  for (int i = 0; i < n; ++i) {
+    int s = cell[i];
+    double delh, over;
+    if (o->head_new[s] >= bott[i]) { delh = head[i] - o->head_new[s]; over = DONE; }
+    else if (head[i] > bott[i]) { delh = head[i] - bott[i]; over = DZERO; }
+    else { delh = DZERO; over = DONE; }
+    double per = o->per_relp[s], rel = o->rel_perm[s];
+    double tran = o->hydf_surf[s] * abyd[i];
+    double deri = -tran * rel;
+    double deri_ks = (per - rel) * o->newper_inv * delh * tran * over;
+    dmat_out[s] = deri + deri_ks;
+  }
+}
+
+/* set_vwell_head (Time_module.f90:1137-1158) with calc_vheadout / calc_vheadin (:1253-1335):
+ * each well's head without pumping is the kr*abyd-weighted mean of its cells' heads; the
+ * pumping rate divided by the total conductance raises it; every cell of the well where
+ * that head or the cell's head lies above the well bottom gets kr*abyd*(whead - head).
+ * rel_perm is the one at head_new, as the reference's array holds it at that point. */
+static void set_vwell_head(orc_t *o) {
+  int N = o->ncalc;
+  memset(o->calc_well, 0, sizeof(double) * N);
+  if (o->nwell == 0) return;
+  double *sr = xc(N, sizeof(double)), *kr = xc(N, sizeof(double)), *al = xc(N, sizeof(double));
+  srat_rperm(o, DZERO, o->head_new, sr, kr, al);
+  for (int w = 0; w < o->nwell; ++w) {
+    double tot_cond = DZERO, tot_flux = DZERO, whead = DZERO;
+    for (int k = o->w_index[w]; k < o->w_index[w + 1]; ++k) {
+      int j = o->w_conn[k];
+      tot_cond = tot_cond + kr[j] * o->w_abyd[k];
+      tot_flux = tot_flux + kr[j] * o->w_abyd[k] * o->head_new[j];
+    }
+    if (tot_cond != DZERO) whead = tot_flux / tot_cond;
+    if (tot_cond != DZERO) {
+      whead = whead + o->w_rate[w] / tot_cond;
+      for (int k = o->w_index[w]; k < o->w_index[w + 1]; ++k) {
+        int j = o->w_conn[k];
+        if (whead > o->w_bott[w] || o->head_new[j] > o->w_bott[w])
+          o->calc_well[j] = o->calc_well[j] + kr[j] * o->w_abyd[k] * (whead - o->head_new[j]);
+      }
+    }
+  }
+  free(sr); free(kr); free(al);
+}
+
 static void calc_func_alp(orc_t *o, const double *infx, double *funcv, const double *alp_old_in) {
   int N = o->ncalc, S = o->ncals;
   double *alp = xc(N, sizeof(double));
@@ -347,6 +425,10 @@ static void calc_func_alp(orc_t *o, const double *infx, double *funcv, const dou
   for (int s = 0; s < S; ++s) recf[s] = o->calc_rech[s];
   /* func_surfterm */
   func_surfterm(o, infx, o->surf_head, surf);
+  /* func_riveterm, func_laketerm */
+  double *rivf = xc(S, sizeof(double)), *lakf = xc(S, sizeof(double));
+  func_riveterm(o, infx, rivf);
+  func_laketerm(o, infx, lakf);
   /* func_sealterm */
   for (int k = 0; k < o->nseal; ++k) {
     int c = o->sea2cal[k], s = o->sea2sea[k];
@@ -354,17 +436,18 @@ static void calc_func_alp(orc_t *o, const double *infx, double *funcv, const dou
     double flow = o->sea_hydf[k] * o->rel_perm[c] * o->sea_abyd[k] * delhead;
     seaf[c] = seaf[c] + flow;
   }
+  /* func_wellterm: welf(j) = calc_well(j) on the well cells, zero elsewhere (calc_well is) */
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < N; ++i) {
     double fs = DZERO;
-    if (i < S) fs = recf[i] + surf[i] + DZERO + DZERO;
-    double f = fs + stof[i] + conf[i] + DZERO + seaf[i];
+    if (i < S) fs = recf[i] + surf[i] + rivf[i] + lakf[i];
+    double f = fs + stof[i] + conf[i] + o->calc_well[i] + seaf[i];
     /* free drainage (extension; appended after the reference terms) */
     if (o->drain_coef[i] != DZERO) f = f + (-(o->drain_coef[i] * o->rel_perm[i]));
     funcv[i] = f;
   }
   o->n_func++;
-  free(alp); free(stof); free(conf); free(seaf); free(recf); free(surf);
+  free(alp); free(stof); free(conf); free(seaf); free(recf); free(surf); free(rivf); free(lakf);
 }
 
 static void calc_func(orc_t *o, const double *infx, double *funcv) { calc_func_alp(o, infx, funcv, NULL); }
@@ -439,6 +522,10 @@ static void make_matrix(orc_t *o, double *diamat, double *lumat) {
     double deri_ks = (o->per_relp[i] - o->rel_perm[i]) * o->newper_inv * delh * tran * over;
     surd[i] = deri_s + deri_ks;
   }
+  /* set_rivebound, set_lakebound */
+  double *rivd = xc(S, sizeof(double)), *lakd = xc(S, sizeof(double));
+  stage_bound(o, o->nriv, o->riv_cell, o->riv_head, o->riv_bott, o->riv_abyd, rivd);
+  stage_bound(o, o->nlak, o->lak_cell, o->lak_head, o->lak_bott, o->lak_abyd, lakd);
   /* set_seabound */
   for (int k = 0; k < o->nseal; ++k) {
     int c = o->sea2cal[k], s = o->sea2sea[k];
@@ -452,13 +539,13 @@ static void make_matrix(orc_t *o, double *diamat, double *lumat) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < N; ++i) {
     double ds = DZERO;
-    if (i < S) ds = surd[i] + DZERO + DZERO;
+    if (i < S) ds = surd[i] + rivd[i] + lakd[i];
     double d = ds + stod[i] + cond[i] + sead[i];
     if (o->drain_coef[i] != DZERO)
       d = d + (-((o->per_relp[i] - o->rel_perm[i]) * o->newper_inv * o->drain_coef[i]));
     diamat[i] = d;
   }
-  free(ss_alp); free(stod); free(cond); free(sead); free(surd);
+  free(ss_alp); free(stod); free(cond); free(sead); free(surd); free(rivd); free(lakd);
 }
 
 static void make_amgmat(orc_t *o);
@@ -1229,6 +1316,8 @@ static int time_loop(orc_t *o, int nsteps, double rech_until, double rech_after,
     for (int s = 0; s < S; ++s) o->calc_rech[s] = o->rech_base[s] * scale;
     o->current_t = (double)(float)(o->current_t + (double)(float)o->delt);
     o->delt_inv = DONE / o->delt;
+    /* update_tstep (Time_module.f90:83-87): well rates after an accepted step or at the start */
+    if ((conv == 1 || o->timestep_num == 0) && o->nwell > 0) set_vwell_head(o);
     /* Newton initial guess (extension): linear extrapolation in time */
     if (o->prm.guess_mode == 1 && o->timestep_num > 0) {
       double ratio = o->delt / o->delt_old1;
@@ -1274,6 +1363,12 @@ static void calc_mass(orc_t *o, double *out9) {
   double *sf = xc(S, sizeof(double));
   func_surfterm(o, o->head_new, o->surf_old, sf);
   for (int s = 0; s < S; ++s) { acc[2] += o->calc_rech[s] * o->delt; acc[4] += sf[s] * o->delt; }
+  double *rv = xc(S, sizeof(double)), *lk = xc(S, sizeof(double));
+  func_riveterm(o, o->head_new, rv);
+  func_laketerm(o, o->head_new, lk);
+  for (int s = 0; s < S; ++s) { acc[5] += rv[s] * o->delt; acc[6] += lk[s] * o->delt; }
+  for (int i = 0; i < N; ++i) acc[3] += o->calc_well[i] * o->delt;
+  free(rv); free(lk);
   for (int k = 0; k < o->nseal; ++k) {
     int c = o->sea2cal[k], s = o->sea2sea[k];
     double dh = o->read_seal[s] - o->head_new[c];
@@ -1288,8 +1383,8 @@ static void calc_mass(orc_t *o, double *out9) {
  * free-drainage outflow of each column's bottom cell, an extension).  Each term is the
  * reference's rate times delt; seam accumulates over the sea faces of a cell
  * (func_sealterm, Calc_function.f90:506-509) into an array zeroed by calc_cell_mas. */
-static void cell_mass(orc_t *o, double *stom, double *conm, double *seam, double *recm, double *surm,
-                      double *drn) {
+static void cell_mass(orc_t *o, double *stom, double *conm, double *seam, double *welm, double *recm, double *surm,
+                      double *rivm, double *lakm, double *drn) {
   int N = o->ncalc, S = o->ncals;
   double *an = xc(N, sizeof(double)), *ao = xc(N, sizeof(double)), *so = xc(N, sizeof(double));
   double *kr = xc(N, sizeof(double));
@@ -1315,6 +1410,11 @@ static void cell_mass(orc_t *o, double *stom, double *conm, double *seam, double
     if (o->drain_coef[i] != DZERO) drn[i % S] = -(o->drain_coef[i] * o->rel_perm[i]) * o->delt;
   func_surfterm(o, o->head_new, o->surf_old, surm);
   for (int s = 0; s < S; ++s) { recm[s] = o->calc_rech[s] * o->delt; surm[s] = surm[s] * o->delt; }
+  memset(rivm, 0, sizeof(double) * S); memset(lakm, 0, sizeof(double) * S);
+  func_riveterm(o, o->head_new, rivm);
+  func_laketerm(o, o->head_new, lakm);
+  for (int s = 0; s < S; ++s) { rivm[s] = rivm[s] * o->delt; lakm[s] = lakm[s] * o->delt; }
+  for (int i = 0; i < N; ++i) welm[i] = o->calc_well[i] * o->delt;
   double *flow = xc(o->nseal > 0 ? o->nseal : 1, sizeof(double));
   for (int k = 0; k < o->nseal; ++k) {
     int c = o->sea2cal[k], s = o->sea2sea[k];
@@ -1401,7 +1501,7 @@ void *orc_create(const msg_grid_t *g, const msg_params_t *p) {
   o->srat_new = xc(N, 8); o->srat_old = xc(N, 8); o->rel_perm = xc(N, 8); o->new_f = xc(N, 8);
   o->per_srat = xc(N, 8); o->per_relp = xc(N, 8); o->slope_rhs = xc(N, 8);
   o->surf_head = xc(S, 8); o->surf_old = xc(S, 8); o->surf_rati = xc(S, 8);
-  o->calc_rech = xc(S, 8); o->rech_base = xc(S, 8);
+  o->calc_rech = xc(S, 8); o->rech_base = xc(S, 8); o->calc_well = xc(N, 8);
   o->len_scal = p->len_scal;
   o->newper = MACHI_EPS * (double)(1.0f / (float)p->len_scal);
   o->newper_inv = DONE / o->newper;
@@ -1536,8 +1636,39 @@ int orc_advance(void *h, int nsteps, double rech_until, double rech_after, msg_r
 
 void orc_calc_mass(void *h, double *out9) { calc_mass((orc_t *)h, out9); }
 void orc_velocity(void *h, double *facev, double *pointv) { outvelc((orc_t *)h, facev, pointv); }
-void orc_cell_mass(void *h, double *sto, double *con, double *sea, double *rec, double *sur, double *drn) {
-  cell_mass((orc_t *)h, sto, con, sea, rec, sur, drn);
+void orc_cell_mass(void *h, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
+                   double *riv, double *lak, double *drn) {
+  cell_mass((orc_t *)h, sto, con, sea, wel, rec, sur, riv, lak, drn);
+}
+
+/* Well, river and lake tables (cells 1-based as the reference stores them). */
+void orc_set_wells(void *h, int nwell, const int *w_index, const int *w_conn, const double *abyd,
+                   const double *bott, const double *rate) {
+  orc_t *o = h;
+  free(o->w_index); free(o->w_conn); free(o->w_abyd); free(o->w_bott); free(o->w_rate);
+  o->nwell = nwell;
+  int nc = nwell > 0 ? w_index[nwell] : 0;
+  o->w_index = xc(nwell + 1, sizeof(int)); o->w_conn = xc(nc + 1, sizeof(int));
+  o->w_abyd = xc(nc + 1, 8); o->w_bott = xc(nwell + 1, 8); o->w_rate = xc(nwell + 1, 8);
+  for (int w = 0; w <= nwell; ++w) o->w_index[w] = nwell > 0 ? w_index[w] : 0;
+  for (int k = 0; k < nc; ++k) { o->w_conn[k] = w_conn[k] - 1; o->w_abyd[k] = abyd[k]; }
+  for (int w = 0; w < nwell; ++w) { o->w_bott[w] = bott[w]; o->w_rate[w] = rate[w]; }
+  memset(o->calc_well, 0, 8 * (size_t)o->ncalc);
+}
+static void set_stage(int n, const int *cell, const double *head, const double *bott, const double *abyd,
+                      int *on, int **oc, double **oh, double **ob, double **oa) {
+  free(*oc); free(*oh); free(*ob); free(*oa);
+  *on = n;
+  *oc = xc(n + 1, sizeof(int)); *oh = xc(n + 1, 8); *ob = xc(n + 1, 8); *oa = xc(n + 1, 8);
+  for (int i = 0; i < n; ++i) { (*oc)[i] = cell[i] - 1; (*oh)[i] = head[i]; (*ob)[i] = bott[i]; (*oa)[i] = abyd[i]; }
+}
+void orc_set_rivers(void *h, int n, const int *cell, const double *head, const double *bott, const double *abyd) {
+  orc_t *o = h;
+  set_stage(n, cell, head, bott, abyd, &o->nriv, &o->riv_cell, &o->riv_head, &o->riv_bott, &o->riv_abyd);
+}
+void orc_set_lakes(void *h, int n, const int *cell, const double *head, const double *bott, const double *abyd) {
+  orc_t *o = h;
+  set_stage(n, cell, head, bott, abyd, &o->nlak, &o->lak_cell, &o->lak_head, &o->lak_bott, &o->lak_abyd);
 }
 
 void orc_vecjacf(void *h, const double *x, const double *v, double *out) { calc_vecjacf((orc_t *)h, x, v, out); }

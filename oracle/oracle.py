@@ -48,7 +48,10 @@ def lib():
         L.orc_init_state.argtypes = [vp, abi.PD, C.c_double]
         L.orc_set_state.argtypes = [vp, abi.PD, abi.PD, abi.PD, abi.PD, C.c_double]
         L.orc_srat_rperm.argtypes = [vp, abi.PD, C.c_double, abi.PD, abi.PD, abi.PD]
-        L.orc_cell_mass.argtypes = [vp] + [abi.PD] * 6
+        L.orc_cell_mass.argtypes = [vp] + [abi.PD] * 9
+        L.orc_set_wells.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PD, abi.PD, abi.PD]
+        L.orc_set_rivers.argtypes = [vp, C.c_int, abi.PI, abi.PD, abi.PD, abi.PD]
+        L.orc_set_lakes.argtypes = [vp, C.c_int, abi.PI, abi.PD, abi.PD, abi.PD]
         L.orc_velocity.argtypes = [vp, abi.PD, abi.PD]
         L.orc_amg_level_sizes.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PI]
         L.orc_amg_level.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
@@ -197,12 +200,33 @@ class Oracle:
         return out
 
     def cell_mass(self):
-        """calc_cell_mas per cell: dict of sto, con, sea [ncalc] and rec, sur, drn [ncals]."""
+        """calc_cell_mas per cell: dict of sto, con, sea, wel [ncalc] and rec, sur, riv, lak, drn [ncals]."""
         N, S = self.prob.ncalc, self.prob.ncals
-        out = dict(sto=np.zeros(N), con=np.zeros(N), sea=np.zeros(N), rec=np.zeros(S), sur=np.zeros(S),
-                   drn=np.zeros(S))
-        lib().orc_cell_mass(C.c_void_p(self.h), *(dptr(out[k]) for k in ("sto", "con", "sea", "rec", "sur", "drn")))
+        keys = (("sto", N), ("con", N), ("sea", N), ("wel", N), ("rec", S), ("sur", S), ("riv", S), ("lak", S),
+                ("drn", S))
+        out = {k: np.zeros(n) for k, n in keys}
+        lib().orc_cell_mass(C.c_void_p(self.h), *(dptr(out[k]) for k, _ in keys))
         return out
+
+    def set_wells(self, well_index, well_conn, abyd, bott, rate):
+        """Well table as set_wellconn leaves it: well_index [nwell+1] prefix offsets, well_conn
+        1-based cells, abyd_well per connection; well_bott and the pumping rate read_well per well."""
+        wi = np.ascontiguousarray(well_index, dtype=np.int32)
+        lib().orc_set_wells(C.c_void_p(self.h), len(wi) - 1, iptr(wi), iptr(np.ascontiguousarray(well_conn, np.int32)),
+                            dptr(np.ascontiguousarray(abyd, np.float64)), dptr(np.ascontiguousarray(bott, np.float64)),
+                            dptr(np.ascontiguousarray(rate, np.float64)))
+
+    def set_rivers(self, cells, head, bott, abyd):
+        """River cells (rive2cals, 1-based surface cells) with stage, bed and area/distance."""
+        self._stage(lib().orc_set_rivers, cells, head, bott, abyd)
+
+    def set_lakes(self, cells, head, bott, abyd):
+        """Lake cells (lake2cals, 1-based surface cells) with stage, bed and area/distance."""
+        self._stage(lib().orc_set_lakes, cells, head, bott, abyd)
+
+    def _stage(self, fn, cells, head, bott, abyd):
+        c = np.ascontiguousarray(cells, np.int32)
+        fn(C.c_void_p(self.h), len(c), iptr(c), *(dptr(np.ascontiguousarray(a, np.float64)) for a in (head, bott, abyd)))
 
     def velocity(self):
         """calc_outvelc: (facev [6, ncalc] face-major, pointv [3, ncalc] x, y, z)."""

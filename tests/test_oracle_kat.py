@@ -832,3 +832,86 @@ def test_velocity_unit_gradient_column():
     assert np.allclose(pv[2, inner], -ks, rtol=1e-12)
     assert not np.any(pv[:2])
     assert fv[5, -1] == -ks                            # free drainage at the bottom, kr = 1
+
+
+def _boundary_tables(p):
+    """A river over three top cells, a lake over one, and two wells of three cells each
+    (vertical, one extracting and one injecting), on a heterogeneous block."""
+    nx, ny, S = p.nx, p.ny, p.ncals
+    top = p.cell_top[:S]
+    riv_cells = np.array([2, nx + 3, 2 * nx + 4])            # 1-based surface cells
+    rs = riv_cells - 1
+    riv = (riv_cells, top[rs] + 0.02, top[rs] - 0.05, np.full(3, 2.5))
+    lk = np.array([S - 1])
+    lak = (lk, top[lk - 1] - 0.01, top[lk - 1] - 0.2, np.array([1.7]))
+    c1 = 1 + (nx // 2) + nx * (ny // 2)                       # a column in the middle
+    c2 = 2 + nx * 1
+    col = lambda c: np.array([c + k * S for k in (1, 2, 3)])
+    wells = (np.array([0, 3, 6]), np.concatenate([col(c1), col(c2)]), np.full(6, 0.8),
+             np.array([float(p.cell_top[-1]) - 1.0, float(p.cell_top[-1]) - 1.0]),
+             np.array([-2.0e-4, 1.0e-4]))
+    return riv, lak, wells
+
+
+def test_river_lake_terms_added_to_residual_and_diagonal():
+    """func_riveterm / func_laketerm enter F on their surface cells only, as
+    hydf_surf * abyd * (stage - head) * kr (head above the bed) or * (stage - bed) (only the
+    stage above), and set_rivebound / set_lakebound add -tran kr + the kr chord to dmat."""
+    p = make_config("hetero", shape=(8, 7, 6), seed=5)
+    o = Oracle(p)
+    o.init_state()
+    rng = np.random.default_rng(2)
+    h = p.cell_top + rng.uniform(-0.3, 0.05, p.ncalc)
+    o.set_state(head_new=h, delt=600.0)
+    f0 = o.calc_func(h)
+    d0, lu0, r0 = o.make_matvec()
+    riv, lak, _ = _boundary_tables(p)
+    o.set_rivers(*riv)
+    o.set_lakes(*lak)
+    f1 = o.calc_func(h)
+    d1, lu1, r1 = o.make_matvec()
+    # newper = epsilon(1._SP) * len_scal_inv, the reciprocal in single precision (Prep_calculation.f90:79)
+    newper = 1.1920928955078125e-07 * float(np.float32(1.0) / np.float32(p.params["len_scal"]))
+    s_, kr, _ = o.srat_rperm(h)
+    _, krp, _ = o.srat_rperm(h, newper)
+    touched = set()
+    for cells, head, bott, abyd in (riv, lak):
+        for c, st, bd, ab in zip(cells, head, bott, abyd):
+            s = c - 1
+            touched.add(s)
+            hy = float(p.ksz[s])
+            if h[s] >= bd:
+                delh, over = st - h[s], 1.0
+            elif st > bd:
+                delh, over = st - bd, 0.0
+            else:
+                delh, over = 0.0, 1.0
+            term = hy * ab * delh * kr[s]
+            assert abs((f1[s] - f0[s]) - term) <= 1e-12 * max(abs(f1[s]), abs(term))
+            tran = hy * ab
+            dd = -tran * kr[s] + (krp[s] - kr[s]) * (1.0 / newper) * delh * tran * over
+            assert abs((d1[s] - d0[s]) - dd) <= 1e-10 * max(abs(d1[s]), abs(dd))
+    rest = np.array([i for i in range(p.ncalc) if i not in touched])
+    assert np.array_equal(f1[rest], f0[rest]) and np.array_equal(d1[rest], d0[rest])
+    assert np.array_equal(lu1, lu0)
+
+
+def test_well_rates_deliver_the_pumping_rate():
+    """set_vwell_head: the virtual well head is set so that the cells' kr*abyd*(whead - h)
+    add up to the pumping rate, so over a step the well volumes of calc_mass are the
+    rates times delt; the step's volumes balance to the accuracy of the Newton solve (its
+    test is on the head change, 1e-8 of max|h|, which leaves ~1e-6 of the volumes here)."""
+    p = make_config("hetero", shape=(8, 7, 6), seed=5)
+    o = Oracle(p)
+    o.init_state()
+    _, _, wells = _boundary_tables(p)
+    o.set_wells(*wells)
+    rc, st = o.advance(nsteps=1)
+    assert rc == 0
+    m = o.calc_mass()
+    delt = st["delt"]
+    assert abs(m[3] - wells[4].sum() * delt) <= 1e-12 * abs(wells[4]).sum() * delt
+    cm = o.cell_mass()
+    assert abs(cm["wel"].sum() - m[3]) <= 1e-14 * abs(m[3]) + 1e-300
+    assert np.count_nonzero(cm["wel"]) == 6
+    assert abs(float(np.sum(m))) <= 1e-5 * (abs(m[2]) + abs(wells[4]).sum() * delt)
