@@ -28,7 +28,7 @@ module msg_gpu
     real(c_float) :: jac_omega, amg_theta, smooth_omega
     integer(c_int32_t) :: sim_type, amg_lag
     real(c_double) :: ini_step, inc_fact, max_step, end_time
-    integer(c_int32_t) :: guess_mode, guess_select, vg_form, pad
+    integer(c_int32_t) :: guess_mode, guess_select, vg_form, jv_mode
   end type
 
   ! One Newton solve (the columns of the reference's convergence log).

@@ -97,7 +97,10 @@ typedef struct msg_params {
                                 1 = the same function with Se^(1/m) = 1/(1+beta) and
                                 beta^m = (alpha|h|)^(n-1): two pow per cell; differs from 0 by
                                 rounding only                                                     */
-  int32_t pad;
+  int32_t jv_mode;           /* J.dh of the line-search slope: 0 = Brown-Saad differencing of F
+                                (calc_vecjacf, the reference: one more residual evaluation per
+                                Newton iteration); 1 = rhs - r, the assembled Jacobian times dh as
+                                BiCGStab's own residual r leaves it (ref_quirks = 0 only)          */
 } msg_params_t;
 
 /* Per-Newton-solve statistics (fields of the reference conv log, Nonlinear_solution.f90:59-63). */
@@ -347,6 +350,12 @@ MSG_API int msg_gpu_cnn_set_weights(msg_cnn_t *cnn, const float *w);
 /* append a training sample from a context right after an accepted step */
 MSG_API int msg_gpu_cnn_collect(msg_cnn_t *cnn, msg_ctx_t *ctx);
 MSG_API int msg_gpu_cnn_nsamples(msg_cnn_t *cnn);
+/* bound the sample store to cap samples (0: unbounded): once full, each collected step
+   replaces a uniformly drawn stored sample with probability cap / (steps collected), so the
+   store stays a uniform sample of every step seen (reservoir sampling; seed seeds the draws) */
+MSG_API int msg_gpu_cnn_set_capacity(msg_cnn_t *cnn, int32_t cap, int32_t seed);
+/* steps offered to msg_gpu_cnn_collect since the capacity was set */
+MSG_API long long msg_gpu_cnn_seen(msg_cnn_t *cnn);
 /* append a sample from host arrays: x [N][16] features, y [N] target, N = nx*ny*nz */
 MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *cnn, int32_t nx, int32_t ny, int32_t nz, const float *x, const float *y);
 /* inference pass of the tensor-core (tcgen05) path on a stored sample; out: N floats.

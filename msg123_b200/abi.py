@@ -52,7 +52,7 @@ class MsgParams(C.Structure):
         ("sim_type", C.c_int32), ("amg_lag", C.c_int32),
         ("ini_step", C.c_double), ("inc_fact", C.c_double), ("max_step", C.c_double),
         ("end_time", C.c_double), ("guess_mode", C.c_int32), ("guess_select", C.c_int32),
-        ("vg_form", C.c_int32), ("pad", C.c_int32),
+        ("vg_form", C.c_int32), ("jv_mode", C.c_int32),
     ]
 
 

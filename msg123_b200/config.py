@@ -88,7 +88,7 @@ def default_params(**kw):
         amg_nlevel=10, amg_coarse_max=2000, amg_sweeps=2, amg_lag=0,
         jac_omega=0.67, amg_theta=0.05, smooth_omega=0.67,
         sim_type=0, ini_step=1800.0, inc_fact=1.0, max_step=3600.0, end_time=1.0e30, guess_mode=0, guess_select=1,
-        vg_form=0,
+        vg_form=0, jv_mode=0,
     )
     p.update(kw)
     return p

@@ -187,7 +187,12 @@ static int run_backtr(msg_ctx *c) {
   // taken before F(head_new) so that the last residual evaluation of the line search is
   // always the one at the accepted head_new (its S and kr stay current; calc_numsol reuses it)
   double *jacvec = c->tmpv;
-  if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) return rc;
+  if (c->prm.jv_mode == 1 && !c->prm.ref_quirks) {
+    // J.dh of the assembled Jacobian: BiCGStab started from dh = 0 and keeps r = rhs - J dh
+    if ((rc = axpby(c, jacvec, c->rhs, -1.0, c->r, n))) return rc;
+  } else if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) {
+    return rc;
+  }
   double dummy;
   if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
   double l2_pnorm;
@@ -608,6 +613,7 @@ int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t
   if (params->maxout_iter < 1 || params->maxinn_iter < 1) { set_error("iteration caps must be >= 1"); return MSG_ERR_ARG; }
   if (params->vg_form != 0 && params->vg_form != 1) { set_error("vg_form must be 0 or 1"); return MSG_ERR_ARG; }
   if (params->precision != 0 && params->precision != 1) { set_error("precision must be 0 or 1"); return MSG_ERR_ARG; }
+  if (params->jv_mode != 0 && params->jv_mode != 1) { set_error("jv_mode must be 0 or 1"); return MSG_ERR_ARG; }
   const void *req[] = {grid->reta, grid->retn, grid->resi, grid->poro, grid->ss, grid->ksx, grid->ksy, grid->ksz,
                        grid->cell_top, grid->cell_vol, grid->dis2face, grid->face_area, grid->surf_top, grid->surf_bott};
   for (auto q : req) if (!q) { set_error("required grid array is NULL"); return MSG_ERR_ARG; }

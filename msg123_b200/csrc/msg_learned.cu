@@ -66,6 +66,12 @@ struct Net {
   double *hpin = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<Sample> data;
+  // bounded sample store: with store_cap > 0, a sample collected when the store is full
+  // replaces a uniformly drawn stored one with probability store_cap / seen (reservoir sampling), so the
+  // store stays a uniform sample of every step collected so far
+  int store_cap = 0;
+  long long seen = 0;
+  unsigned long long rs = 0x2545F4914F6CDD1Dull;
 };
 
 }  // namespace msg
@@ -614,21 +620,54 @@ MSG_API int msg_gpu_cnn_collect(msg_cnn_t *h, msg_ctx_t *c) {
   double s = std::sqrt(ss / c->N);
   if (!(s > 0.0)) return MSG_OK;   // no motion: nothing to learn from this step
   double ratio = c->delt / c->delt_old1;
+  Net &n = h->net;
+  n.seen++;
+  long long slot = -1;                       // -1: append
+  if (n.store_cap > 0 && (long long)n.data.size() >= n.store_cap) {
+    n.rs ^= n.rs << 13; n.rs ^= n.rs >> 7; n.rs ^= n.rs << 17;
+    long long r = (long long)(n.rs % (unsigned long long)n.seen);
+    if (r >= n.store_cap) return MSG_OK;     // not kept
+    slot = r;
+  }
   Sample smp;
   smp.g = Grid3{c->nx, c->ny, c->nz, c->nxy, c->N};
-  MSG_CUDA(cudaMalloc(&smp.x, (size_t)c->N * kC * 2));
-  MSG_CUDA(cudaMalloc(&smp.y, (size_t)c->N * 4));
+  if (slot >= 0 && n.data[slot].g.N == c->N) {
+    smp.x = n.data[slot].x; smp.y = n.data[slot].y;       // same size: reuse the buffers
+  } else {
+    MSG_CUDA(cudaMalloc(&smp.x, (size_t)c->N * kC * 2));
+    MSG_CUDA(cudaMalloc(&smp.y, (size_t)c->N * 4));
+  }
   k_features<false><<<(c->N + 255) / 256, 256, 0, c->stream>>>(feat_args(c, 1.0 / s, ratio), smp.x, 0);
   MSG_CHECK_LAUNCH();
   k_target<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->head_new, c->head_old, c->head_old2, ratio, 1.0 / s,
                                                      smp.y);
   MSG_CHECK_LAUNCH();
   MSG_CUDA(cudaStreamSynchronize(c->stream));
-  h->net.data.push_back(smp);
+  if (slot < 0) {
+    n.data.push_back(smp);
+  } else {
+    if (n.data[slot].x != smp.x) {
+      MSG_CUDA(cudaStreamSynchronize(n.stream));        // training may still read the old one
+      cudaFree(n.data[slot].x); cudaFree(n.data[slot].y);
+    }
+    n.data[slot] = smp;
+  }
   return MSG_OK;
 }
 
 MSG_API int msg_gpu_cnn_nsamples(msg_cnn_t *h) { return h ? (int)h->net.data.size() : 0; }
+
+// Bound the sample store to `cap` samples (0: unbounded) kept by reservoir sampling over the
+// collected steps; `seed` seeds the replacement draws.  Existing samples are kept.
+MSG_API int msg_gpu_cnn_set_capacity(msg_cnn_t *h, int32_t cap, int32_t seed) {
+  if (!h || cap < 0) return MSG_ERR_ARG;
+  h->net.store_cap = cap;
+  h->net.seen = (long long)h->net.data.size();
+  h->net.rs = 0x2545F4914F6CDD1Dull ^ ((unsigned long long)(seed + 1) * 0x9E3779B97F4A7C15ull);
+  return MSG_OK;
+}
+// Steps offered to msg_gpu_cnn_collect since the capacity was set (kept or not).
+MSG_API long long msg_gpu_cnn_seen(msg_cnn_t *h) { return h ? h->net.seen : 0; }
 
 // Load a sample from host arrays (x: [N][16] float features, y: [N] target).
 MSG_API int msg_gpu_cnn_add_sample(msg_cnn_t *h, int32_t nx, int32_t ny, int32_t nz, const float *x, const float *y) {

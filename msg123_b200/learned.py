@@ -31,6 +31,9 @@ def _lib():
         L.msg_gpu_cnn_set_weights.argtypes = [vp, abi.PF]
         L.msg_gpu_cnn_collect.argtypes = [vp, vp]
         L.msg_gpu_cnn_nsamples.argtypes = [vp]
+        L.msg_gpu_cnn_set_capacity.argtypes = [vp, C.c_int32, C.c_int32]
+        L.msg_gpu_cnn_seen.argtypes = [vp]
+        L.msg_gpu_cnn_seen.restype = C.c_longlong
         L.msg_gpu_cnn_add_sample.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, abi.PF, abi.PF]
         L.msg_gpu_cnn_loss_grad.argtypes = [vp, C.c_int32, abi.PD, abi.PF, abi.PF]
         L.msg_gpu_cnn_infer.argtypes = [vp, C.c_int32, abi.PF]
@@ -80,6 +83,14 @@ class Cnn:
 
     def nsamples(self):
         return _lib().msg_gpu_cnn_nsamples(self.h)
+
+    def set_capacity(self, cap, seed=0):
+        """Keep at most `cap` samples, a uniform (reservoir) sample of every step collected."""
+        _check(_lib().msg_gpu_cnn_set_capacity(self.h, int(cap), int(seed)), "cnn_set_capacity")
+
+    def seen(self):
+        """Steps offered to collect() since the capacity was set."""
+        return int(_lib().msg_gpu_cnn_seen(self.h))
 
     def add_sample(self, shape, x, y):
         nx, ny, nz = shape

@@ -80,6 +80,7 @@ typedef struct orc {
   int nlevel;
   orc_level lev[16];
   double *slope_rhs;         /* vector the line-search slope reads (Q2) */
+  double *lin_r;             /* BiCGStab's last residual rhs - A x (jv_mode = 1) */
   /* time module */
   double current_t, delt_old1, delt_old2;   /* current_t kept as float value (real(SP)) */
   int timestep_num, last_conv, last_out, amg_age, amg_force;
@@ -681,6 +682,7 @@ static void solve_bicgs(orc_t *o, double *inx) {
     sk0 = sk;
   }
   if (o->in_iter > o->prm.maxinn_iter) o->in_iter = o->prm.maxinn_iter;
+  if (o->lin_r) memcpy(o->lin_r, resi, sizeof(double) * n);
   free(d); free(z); free(p); free(v); free(rs); free(t); free(resi);
 }
 
@@ -1126,7 +1128,12 @@ static void run_backtr(orc_t *o) {
   double *jacvec = xc(n, sizeof(double));
   calc_func(o, o->head_new, o->new_f);
   double l2_pnorm = l2norm2(o->head_change, n);
-  calc_vecjacf(o, o->head_pre, o->head_change, jacvec);
+  if (o->prm.jv_mode == 1 && !o->prm.ref_quirks) {
+    /* extension: J dh of the assembled Jacobian, rhs - r as BiCGStab (from dh = 0) leaves r */
+    for (int i = 0; i < n; ++i) jacvec[i] = o->lev[0].rhs[i] + (-1.0) * o->lin_r[i];
+  } else {
+    calc_vecjacf(o, o->head_pre, o->head_change, jacvec);
+  }
   double sql2_pnorm = sqrt(l2_pnorm);
   if (sql2_pnorm > o->maxstep) {
     maxpnorm = o->maxstep / sql2_pnorm;
@@ -1499,7 +1506,7 @@ void *orc_create(const msg_grid_t *g, const msg_params_t *p) {
   o->head_new = xc(N, 8); o->head_old = xc(N, 8); o->head_pre = xc(N, 8); o->head_change = xc(N, 8);
   o->head_old2 = xc(N, 8);
   o->srat_new = xc(N, 8); o->srat_old = xc(N, 8); o->rel_perm = xc(N, 8); o->new_f = xc(N, 8);
-  o->per_srat = xc(N, 8); o->per_relp = xc(N, 8); o->slope_rhs = xc(N, 8);
+  o->per_srat = xc(N, 8); o->per_relp = xc(N, 8); o->slope_rhs = xc(N, 8); o->lin_r = xc(N, 8);
   o->surf_head = xc(S, 8); o->surf_old = xc(S, 8); o->surf_rati = xc(S, 8);
   o->calc_rech = xc(S, 8); o->rech_base = xc(S, 8); o->calc_well = xc(N, 8);
   o->len_scal = p->len_scal;
@@ -1523,7 +1530,7 @@ void orc_destroy(void *h) {
                   o->surf_area, o->rech_area, o->hydf_surf, o->abyd_surf, o->surf_dis, o->surf_top, o->surf_bott,
                   o->surf_reli, o->surf_parm, o->calc_rech, o->rech_base, o->drain_coef, o->head_new, o->head_old,
                   o->head_pre, o->head_change, o->srat_new, o->srat_old, o->rel_perm, o->surf_head, o->surf_old,
-                  o->surf_rati, o->new_f, o->per_srat, o->per_relp, o->slope_rhs, o->head_old2};
+                  o->surf_rati, o->new_f, o->per_srat, o->per_relp, o->slope_rhs, o->head_old2, o->lin_r};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   free(o);
 }

@@ -349,3 +349,27 @@ def test_time_loop_restated(name, kw, nsteps, rech_until):
         assert r1[k] == r2[k], k
     assert r1["current_t"] == t2 and r1["delt"] == d2
     assert np.array_equal(o1.get_state()["head_new"], h2)
+
+
+def test_jv_mode_slope_from_linear_residual():
+    """Oracle with jv_mode = 1: the line-search slope comes from the assembled Jacobian
+    (rhs - r after BiCGStab) instead of a difference of residuals, so one residual
+    evaluation fewer per Newton iteration; the converged heads stay within the Newton
+    tolerance of the jv_mode = 0 run."""
+    from msg123_b200.config import make_config
+    from oracle.oracle import Oracle
+    p = make_config("hetero", shape=(12, 10, 8), seed=4)
+    ov = dict(precon_type=1, ref_quirks=0, amg_lag=1, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    runs = {}
+    for jv in (0, 1):
+        o = Oracle(p, jv_mode=jv, **ov)
+        o.init_state()
+        rc, st = o.advance(nsteps=3)
+        assert rc == 0
+        runs[jv] = (o.get_state()["head_new"], st, o.counters()["func"])
+        o.close()
+    h0, s0, f0 = runs[0]
+    h1, s1, f1 = runs[1]
+    assert np.max(np.abs(h1 - h0)) / np.max(np.abs(h0)) <= 1e-8
+    # calc_vecjacf evaluates F once more per Newton iteration with jv_mode = 0
+    assert f1 < f0
