@@ -83,6 +83,9 @@ module msg_gpu
     integer(c_int) function msg_gpu_get_state(ctx, hn, ho, sn, so, sh) bind(C)
       import; type(c_ptr), value :: ctx; real(c_double), intent(out) :: hn(*), ho(*), sn(*), so(*), sh(*)
     end function
+    integer(c_int) function msg_gpu_copy_state(dst, src) bind(C)
+      import; type(c_ptr), value :: dst, src
+    end function
     integer(c_int) function msg_gpu_set_recharge(ctx, rech) bind(C)
       import; type(c_ptr), value :: ctx; real(c_double), intent(in) :: rech(*)
     end function
