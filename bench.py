@@ -10,15 +10,17 @@ time level (msg_gpu_copy_state) and covers the same window:
 
 * value        : mixed precision + learned initial guess (FP32/BF16 V-cycle, FP64 Krylov
                  and Newton, AMG hierarchy rebuilt every 4 time steps, CNN guess with
-                 extrapolation fallback); cells x K accepted steps / device time (CUDA
-                 events on the library stream).  It ends at simulated time T.
+                 extrapolation fallback, line-search slope from BiCGStab's residual);
+                 cells x K accepted steps / device time (CUDA events on the library
+                 stream).  It ends at simulated time T.
 * arms         : the same window up to T with one change at a time -- mixed precision
                  with the plain extrapolation (no network), FP64 with the extrapolation
                  and the same AMG reuse, and plain FP64 (the reference's method on the
                  GPU: AMG rebuilt at every Newton iteration, Newton from the previous
                  head), each with Newton/Krylov counts, rejections and simulated seconds.
                  The head and the stored water volume of the value path are compared with
-                 the plain FP64 arm at T.
+                 the plain FP64 method run from the same state on the value path's own time
+                 steps (so both solve the same discrete equations).
 * e2e          : the value path over the same K steps through the public C ABI with the
                  state in pinned host memory (set_state / advance / get_state each step,
                  copies inside the timed region, host wall clock).
@@ -225,8 +227,9 @@ def make_problem(args, rank):
 
 
 # value path: mixed precision, learned guess used directly (a failed solve from it is redone
-# from the plain extrapolation), AMG hierarchy kept for 4 time steps, two-pow Mualem kr
-FAST = dict(precision=1, amg_lag=4, guess_mode=2, guess_select=0, vg_form=1)
+# from the plain extrapolation), AMG hierarchy kept for 4 time steps, two-pow Mualem kr,
+# line-search slope from BiCGStab's residual
+FAST = dict(precision=1, amg_lag=4, guess_mode=2, guess_select=0, vg_form=1, jv_mode=1)
 # one change at a time from the value path, over the same window
 ARMS = (("mixed_extrapolation", dict(FAST, guess_mode=1)),
         ("fp64_extrapolation", dict(FAST, precision=0, guess_mode=1)),
@@ -245,8 +248,8 @@ def workload_config(args, prob):
             "solver": "Newton (Eisenstat-Walker, cubic line search) + BiCGStab + smoothed-aggregation AMG",
             "value_path": "mixed precision (FP32 V-cycle, BF16 coarse operators, FP64 Krylov/Newton/coarse LU) + "
                           "learned initial guess (guess_select %d), AMG hierarchy rebuilt every %d time steps, "
-                          "two-pow form of Mualem kr (vg_form %d)" % (FAST["guess_select"], FAST["amg_lag"],
-                                                                      FAST["vg_form"]),
+                          "two-pow form of Mualem kr (vg_form %d), line-search slope from BiCGStab's residual "
+                          "(jv_mode %d)" % (FAST["guess_select"], FAST["amg_lag"], FAST["vg_form"], FAST["jv_mode"]),
             "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} after {args.warmup} warm-up steps of "
                       "the value path; every arm starts from the same saved time level",
             "newton_tol": "max|dh| <= 1e-8 max|h|",
@@ -452,16 +455,6 @@ def main():
             g = prep_arm(prob, kw, gw, cnn, end_time=t_end)
             sta, msa, _ = run_arm(g, 4 * K)
             arms[name] = arm_stats(prob, sta, msa, dist)
-            if name == "plain_fp64":
-                head_d = g.get_state(out={"head_new": np.zeros(prob.ncalc)})["head_new"]
-                vol_d = water_volume(g, head_d)
-                inflow = inflow_volume(prob, t_start, t_end)
-                errors = {"against": "plain_fp64 at the same simulated time",
-                          "simulated_s": sta["current_t"],
-                          "head_rel": reduce(dist, float(np.max(np.abs(head_a - head_d)) / np.max(np.abs(head_d))),
-                                             "max"),
-                          "stored_water_rel_inflow": reduce(dist, abs(vol_a - vol_d) / inflow, "max"),
-                          "inflow_volume": inflow}
             g.close()
     for a in list(arms.values()) + [value_arm]:
         a["simulated_s_per_s"] = (a["simulated_s"] - t_start) / (a["ms_per_step"] * max(a["accepted"], 1) * 1e-3)
@@ -478,6 +471,7 @@ def main():
         ge.get_state(out={"head_new": heads[0], "head_old": heads[1], "srat_new": sat, "surf_head": surf})
         barrier(dist)
         acc = newton = 0
+        dts = []
         t0 = time.perf_counter()
         for _ in range(K):
             ge.set_state(head_new=heads[0], head_old=heads[1], srat_old=sat, surf_head=surf)
@@ -486,6 +480,7 @@ def main():
             heads.reverse()
             acc += st2["accepted"]
             newton += st2["newton_total"]
+            dts.append(st2["delt"])
         te = reduce(dist, time.perf_counter() - t0, "max")
         e2e = {"value": reduce(dist, float(prob.ncalc * acc), "sum") / te, "unit": "cell-timesteps/s",
                "h2d_bytes_per_step": 3 * N * 8 + S * 8, "d2h_bytes_per_step": 2 * N * 8 + S * 8,
@@ -495,6 +490,24 @@ def main():
                        "msg_gpu_advance / msg_gpu_get_state (head_new, srat_new, surf_head), pinned host "
                        "buffers, host wall clock"}
         ge.close()
+        # ---- errors of the value path against plain FP64 on the same time steps ----------
+        # (the reference's method from the same state, each step forced to the value path's
+        # dt, so both solve the same discrete equations and differ by their arithmetic only)
+        if not args.no_arms:
+            gf = GpuSolver(prob, **dict(ARMS[-1][1], sim_type=0, inc_fact=1.0))
+            gf.copy_state_from(gw)
+            for dt in dts:
+                gf.set_state(delt=dt)
+                gf.advance(nsteps=1)
+            head_d = gf.get_state(out={"head_new": np.zeros(prob.ncalc)})["head_new"]
+            vol_d = water_volume(gf, head_d)
+            inflow = inflow_volume(prob, t_start, t_end)
+            errors = {"against": "plain FP64 (reference method) on the value path's own time steps",
+                      "steps": len(dts),
+                      "head_rel": reduce(dist, float(np.max(np.abs(head_a - head_d)) / np.max(np.abs(head_d))), "max"),
+                      "stored_water_rel_inflow": reduce(dist, abs(vol_a - vol_d) / inflow, "max"),
+                      "inflow_volume": inflow}
+            gf.close()
     gw.close()
 
     # ---- CPU baseline: the reference's method on the host cores, and on the GPU beside it --

@@ -729,8 +729,12 @@ struct Dia32 {
   const float *d, *lu;
 };
 
-__device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x) {
-  int iz = i / A.nxy, rem = i - iz * A.nxy, iy = rem / A.nx, ix = rem - iy * A.nx;
+
+// Row i of the FP32 level-1 operator (DIA: diagonal, then the up, north, west, east, south
+// and down off-diagonals) times x, with the cell's grid coordinates given by a 3D launch (x
+// from the thread, y from the block's y, the layer from the block's z): no integer
+// division per cell.
+__device__ __forceinline__ float dia_row3_f(const Dia32 &A, int i, int ix, int iy, int iz, const float *x) {
   const size_t N = A.N;
   float t = A.d[i] * x[i];
   if (iz > 0) t += A.lu[0 * N + i] * x[i - A.nxy];
@@ -740,6 +744,22 @@ __device__ __forceinline__ float dia_row_f(const Dia32 &A, int i, const float *x
   if (iy < A.ny - 1) t += A.lu[4 * N + i] * x[i + A.nx];
   if (iz < A.nz - 1) t += A.lu[5 * N + i] * x[i + A.nxy];
   return t;
+}
+// Fine-level Jacobi sweep (y = x + w (b - A x) / d) and residual (b - A x) over a 3D grid
+// of (32, B/32) thread blocks.
+template <typename TY>
+__global__ void k_jac_dia3(Dia32 A, const float *__restrict__ b, float w, const float *__restrict__ x, TY *y) {
+  const int ix = blockIdx.x * 32 + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y, iz = blockIdx.z;
+  if (ix >= A.nx || iy >= A.ny) return;
+  const int i = ix + A.nx * (iy + A.ny * iz);
+  float r = b[i] - dia_row3_f(A, i, ix, iy, iz, x);
+  y[i] = (TY)(x[i] + (w * r) / A.d[i]);
+}
+__global__ void k_res_dia3(Dia32 A, const float *__restrict__ b, const float *__restrict__ x, float *r) {
+  const int ix = blockIdx.x * 32 + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y, iz = blockIdx.z;
+  if (ix >= A.nx || iy >= A.ny) return;
+  const int i = ix + A.nx * (iy + A.ny * iz);
+  r[i] = b[i] - dia_row3_f(A, i, ix, iy, iz, x);
 }
 
 template <typename TB>
@@ -759,17 +779,6 @@ __global__ void k_jac_first_b(int n, const double *b, const float *d, float w, f
 }
 __global__ void k_b2f(int n, const double *b, float *bf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) bf[i] = (float)b[i];
-}
-template <typename TY>
-__global__ void k_jac_dia_f(Dia32 A, const float *b, float w, const float *x, TY *y) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x) {
-    float r = b[i] - dia_row_f(A, i, x);
-    y[i] = (TY)(x[i] + (w * r) / A.d[i]);
-  }
-}
-__global__ void k_res_dia_f(Dia32 A, const float *b, const float *x, float *r) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.N; i += gridDim.x * blockDim.x)
-    r[i] = b[i] - dia_row_f(A, i, x);
 }
 // Coarse levels: four lanes per row (lane q takes entries q, q+4, ... of the row; quad
 // shuffle sum), so a warp keeps eight rows' loads in flight instead of 32 serial walks.
@@ -1374,6 +1383,9 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   const bool single = (A->lv.size() == 1);
   const int bs = c->blk_smooth > 0 ? c->blk_smooth : kThreads;
   const int gs = (n + bs - 1) / bs;
+  // stencil sweeps: 3D grid, 32 cells of a row per warp, bs / 32 rows per block
+  const int by = std::max(bs / 32, 1);
+  const dim3 b3(32, by), g3((c->nx + 31) / 32, (c->ny + by - 1) / by, c->nz);
   float *cur = A->x0f, *oth = A->t0f, *bf = A->b0f;
   if (sw == 0) {
     MSG_CUDA(cudaMemsetAsync(cur, 0, (size_t)n * 4, s));
@@ -1383,14 +1395,14 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
     k_jac_first_b<<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur, bf);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
+      k_jac_dia3<float><<<g3, b3, 0, s>>>(D, bf, w, cur, oth);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!single) {
     AmgLevel &C = A->lv[1];
-    k_res_dia_f<<<gs, bs, 0, s>>>(D, bf, cur, A->r0f);
+    k_res_dia3<<<g3, b3, 0, s>>>(D, bf, cur, A->r0f);
     MSG_CHECK_LAUNCH();
     k_restrict_f<<<grid4(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
     MSG_CHECK_LAUNCH();
@@ -1401,11 +1413,11 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
   }
   for (int k = 0; k < sw; ++k) {
     if (k == sw - 1) {   // the last sweep writes the FP64 output
-      k_jac_dia_f<double><<<gs, bs, 0, s>>>(D, bf, w, cur, z);
+      k_jac_dia3<double><<<g3, b3, 0, s>>>(D, bf, w, cur, z);
       MSG_CHECK_LAUNCH();
       return MSG_OK;
     }
-    k_jac_dia_f<float><<<gs, bs, 0, s>>>(D, bf, w, cur, oth);
+    k_jac_dia3<float><<<g3, b3, 0, s>>>(D, bf, w, cur, oth);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }

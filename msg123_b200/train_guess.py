@@ -1,7 +1,8 @@
 """Train the learned Newton initial guess on steps the GPU solver generates.
 
-Recipe (train_stream, the default): heterogeneous fields of 128x128x48 cells (the block
-generator with sigma_lnK drawn in [0.5, 1.5]), each advanced over a whole event -- the
+Recipe (train_stream, the default): heterogeneous fields of 128x128x96 cells (the block
+generator with sigma_lnK drawn in [0.5, 1.5]; the 25.2M-cell workload's depth, layer
+thickness and water table), each advanced over a whole event -- the
 rain and the drainage after it -- by the solver settings of the value path with the plain
 extrapolation guess (mixed precision, AMG kept for 4 steps, two-pow kr, adaptive dt);
 every accepted step (features before the step, the head increment after it) is one
@@ -11,7 +12,7 @@ the project's own forward/backward kernels follow each collected step, then a la
 over the store.  Writes msg123_b200/weights/guess_cnn.npy (float32, msg_gpu_cnn_nparam
 values).  `train` is the earlier fixed-set recipe (all samples kept, trained afterwards).
 
-    python -m msg123_b200.train_guess [--fields 500] [--steps 40] [--cap 1200]
+    python -m msg123_b200.train_guess [--fields 400] [--steps 50] [--cap 1000]
 """
 import argparse
 import json
@@ -53,10 +54,10 @@ def train(fields=12, steps=16, iters=2400, seed=0, shape=(128, 128, 48), out=WEI
     return info
 
 
-SOLVER = dict(guess_mode=1, precision=1, amg_lag=4, vg_form=1)
+SOLVER = dict(guess_mode=1, precision=1, amg_lag=4, vg_form=1, jv_mode=1)
 
 
-def train_stream(fields=500, steps=40, cap=1200, iters_per_step=2, final_iters=3000, seed=0, shape=(128, 128, 48),
+def train_stream(fields=400, steps=50, cap=1000, iters_per_step=2, final_iters=3000, seed=0, shape=(128, 128, 96),
                  lr=(2e-3, 5e-4), out=WEIGHTS, log=None, init=None):
     """Streaming recipe: fields x steps generated samples, `iters_per_step` AdamW steps after
     each (learning rate decaying geometrically from lr[0] to lr[1]), then `final_iters` over
@@ -89,6 +90,9 @@ def train_stream(fields=500, steps=40, cap=1200, iters_per_step=2, final_iters=3
         if log and (k + 1) % 25 == 0:
             print(json.dumps(dict(fields=k + 1, samples=done, store=cnn.nsamples(), solve_s=round(t_solve, 1),
                                   train_s=round(t_train, 1))), flush=True)
+        if out and (k + 1) % 100 == 0:             # a checkpoint, so a cut-off run still leaves weights
+            os.makedirs(os.path.dirname(out) or ".", exist_ok=True)
+            np.save(out, cnn.get_weights())
     t0 = time.time()
     last = cnn.train(iters=final_iters, lr=lr[1], weight_decay=1e-5, seed=seed + 17)
     t_train += time.time() - t0
@@ -113,9 +117,9 @@ def load(cnn, path=WEIGHTS):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--fields", type=int, default=500)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--cap", type=int, default=1200)
+    ap.add_argument("--fields", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--cap", type=int, default=1000)
     ap.add_argument("--iters-per-step", type=int, default=2)
     ap.add_argument("--final-iters", type=int, default=3000)
     ap.add_argument("--out", default=WEIGHTS)

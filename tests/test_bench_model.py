@@ -133,7 +133,8 @@ class _FakeSolver:
 
 @pytest.mark.parametrize("extra", [["--no-cpu", "--no-arms", "--no-e2e"],
                                    ["--cpu-shape", "8x8x4", "--no-e2e"],
-                                   ["--no-cpu", "--no-arms"]])
+                                   ["--no-cpu", "--no-arms"],
+                                   ["--no-cpu"]])
 def test_bench_main_dry_run(monkeypatch, capsys, extra):
     """bench.main on the CPU with stand-ins for the CUDA solver and the network: the JSON
     line carries every key of the contract, with values derived from the stand-ins."""
@@ -165,8 +166,9 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
     if "--no-arms" not in extra:                      # every arm stops at the value path's end time
         for name in ("mixed_extrapolation", "fp64_extrapolation", "plain_fp64", "value"):
             assert line["arms"][name]["simulated_s"] == 3000.0
-        assert line["errors_vs_fp64"]["head_rel"] == 0.0
         assert line["speedup_over_plain_fp64"] == pytest.approx(1.0)
+    if "--no-arms" not in extra and "--no-e2e" not in extra:   # FP64 on the value path's own steps
+        assert line["errors_vs_fp64"]["head_rel"] == 0.0 and line["errors_vs_fp64"]["steps"] == 2
     if "--no-e2e" not in extra:                       # pinned host state in and out every step
         e = line["e2e"]
         assert e["h2d_bytes_per_step"] == 3 * 256 * 8 + 64 * 8 and e["d2h_bytes_per_step"] == 2 * 256 * 8 + 64 * 8

