@@ -43,11 +43,14 @@ def check_heads(p, ov, steps, hg, ho, sg, so):
     g.init_state(); t.init_state()
     rg, sgt = g.advance(nsteps=steps)
     rt, stt = t.advance(nsteps=steps)
-    assert rg == rt == 0 and sgt["current_t"] == stt["current_t"] == sg["current_t"]
+    # the tight pair may take other time steps than the criteria-1e-8 pair (a step the
+    # looser run rejected at 20 iterations converges within 60), but the same as each other
+    assert rg == rt == 0 and sgt["current_t"] == stt["current_t"]
     hgt, ht = g.get_state()["head_new"], t.get_state()["head_new"]
+    same_t = sgt["current_t"] == sg["current_t"]
     print("Newton counts differ at criteria 1e-8: gpu", sg["newton_total"], "oracle", so["newton_total"],
           "(gpu vs oracle", rel(hg, ho), ") -> at criteria 1e-10: gpu vs oracle", rel(hgt, ht),
-          "; the criteria-1e-8 runs from it: gpu", rel(hg, ht), "oracle", rel(ho, ht))
+          *(("; the criteria-1e-8 runs from it: gpu", rel(hg, ht), "oracle", rel(ho, ht)) if same_t else ()))
     assert rel(hgt, ht) <= 1e-8
     g.close(); t.close()
     return rel(hgt, ht)

@@ -132,12 +132,15 @@ def test_reference_amg_mode_run():
 
 def test_ensemble_members_against_oracle():
     """Three members advanced together by the batched driver (mixed precision, AMG kept for
-    4 steps, extrapolated guess), each against the FP64 oracle solved to criteria 1e-11 on
-    the member's own field at the same times: heads within 1e-8."""
+    4 steps, extrapolated guess), each against the FP64 oracle solved to criteria 1e-10 on
+    the member's own field at the same times: heads within 1e-8.  The members are small
+    ones (for the oracle's time) whose tight-tolerance oracle run takes the same time steps:
+    member 31 (sigma_lnK 1.38) rejects its second step even at 60 Newton iterations with
+    criteria 1e-10, so no same-time comparison exists for it."""
     from msg123_b200.ensemble import Ensemble, ENSEMBLE
-    seeds = [20, 29, 31]                        # 219k, 209k and 160k cells
+    seeds = [20, 29, 35]                        # 219k, 209k and 230k cells
     # the first step from the hydrostatic start takes more than the default 20 Newton
-    # iterations at criteria 1e-11; both sides get the same cap, so no step is rejected
+    # iterations at criteria 1e-10; both sides get the same cap, so no step is rejected
     sched = dict(sim_type=0, inc_fact=1.1, ini_step=600.0, maxout_iter=60)
     ens = Ensemble(seeds=seeds, **sched)
     ens.init_state()
@@ -145,13 +148,13 @@ def test_ensemble_members_against_oracle():
     assert all(s["status"] == 0 and s["accepted"] == 4 and s["rejected"] == 0 for s in stats)
     for k, seed in enumerate(seeds):
         p = make_member(seed, **sched)
-        o = Oracle(p, **dict(ENSEMBLE, precision=0, amg_lag=1, criteria=1e-11))
+        o = Oracle(p, **dict(ENSEMBLE, precision=0, amg_lag=1, criteria=1e-10))
         o.init_state()
         ro, so = o.advance(nsteps=4)
         assert ro == 0 and so["current_t"] == stats[k]["current_t"]
         err = relmax(ens.members[k].get_state()["head_new"], o.get_state()["head_new"])
         print(f"member {seed} ({p.nx}x{p.ny}x{p.nz}): gpu newton {stats[k]['newton_total']}, "
-              f"oracle(1e-11) newton {so['newton_total']}, head rel {err:.2e}")
+              f"oracle(1e-10) newton {so['newton_total']}, head rel {err:.2e}")
         assert err <= HEAD_TOL
         o.close()
     ens.close()

@@ -97,22 +97,23 @@ def test_training_lowers_loss():
     assert l1 < 0.5 * l0
 
 
-@pytest.mark.parametrize("shape,seed", [((96, 96, 40), 999), ((128, 128, 48), 998)])
+@pytest.mark.parametrize("shape,seed", [((96, 96, 96), 999), ((128, 128, 96), 998)])
 def test_learned_guess_newton_gain(shape, seed):
-    """Shipped weights (msg123_b200/train_guess.py, 128x128x48 training fields) on held-out
-    fields: Newton iterations per step from the reference's previous-head start, from the
-    plain extrapolation, and from the learned guess."""
+    """Shipped weights (msg123_b200/train_guess.py: 20,000 steps generated on 128x128x96
+    fields of seeds 5000-5399, rain and drainage) on held-out fields of the same generator:
+    Newton iterations per step over 24 steps from the reference's previous-head start, from
+    the plain extrapolation and from the learned guess (used directly, extrapolation
+    fallback), the value path's other settings alike."""
     from msg123_b200.learned import Cnn, newton_per_step
     from msg123_b200.train_guess import load
-    kw = dict(amg_lag=1, precision=1)
+    kw = dict(amg_lag=4, precision=1, vg_form=1, jv_mode=1, guess_select=0)
     cnn = load(Cnn(seed=0))
-    test = make_config("hetero", shape=shape, seed=seed)
-    n0, s0, _ = newton_per_step(test, 12, guess_mode=0, **kw)
-    n1, s1, _ = newton_per_step(test, 12, guess_mode=1, **kw)
-    n2, s2, fb = newton_per_step(test, 12, cnn=cnn, guess_mode=2, **kw)
-    print(f"{shape} Newton/step previous-head {n0:.2f} extrapolation {n1:.2f} learned {n2:.2f} "
-          f"(fallbacks, rejected {fb})")
-    assert s2["accepted"] == 12
+    test = make_config("hetero", shape=shape, seed=seed, sigma=1.5)
+    n0, s0, _ = newton_per_step(test, 24, guess_mode=0, **kw)
+    n1, s1, _ = newton_per_step(test, 24, guess_mode=1, **kw)
+    n2, s2, fb = newton_per_step(test, 24, cnn=cnn, guess_mode=2, **kw)
+    print(f"{shape} Newton/step previous-head {n0:.2f} ({s0['current_t']:.0f} s) extrapolation {n1:.2f} "
+          f"({s1['current_t']:.0f} s) learned {n2:.2f} ({s2['current_t']:.0f} s) (fallbacks, rejected {fb})")
+    assert s2["accepted"] == 24
     assert n1 < n0
-    assert n2 < n0                 # gain over the reference's start from the previous head
-    assert n2 <= n1 * 1.1          # and no loss against the plain extrapolation
+    assert n2 < n1                 # the network improves on the plain extrapolation
