@@ -24,6 +24,14 @@ def system(shape=(24, 20, 16), seed=6, delt=3600.0, **kw):
     return p, o, d, lu, r
 
 
+# Run tests use 600-s steps.  With 1800-s steps from the dry hydrostatic start of these
+# 32x28x16 blocks the first steps meet the seepage switch (the surface term is not
+# differentiable where h = surf_top) and Newton with the reference's step-size test can
+# stagnate in the line search: on the seed-14 block the oracle's own runs at criteria
+# 1e-10 and 1e-12 end 1.8e-8 apart, so no run there pins 1e-8.  At 600 s the criteria-1e-8
+# run lies within 2e-9 of the criteria-1e-12 run (seeds 12 and 14).
+
+
 def check_heads(p, ov, steps, hg, ho, sg, so):
     """Heads of a GPU run (hg) and an oracle run (ho) of the same method and time steps.
     When both take the same Newton iterations they follow the same path up to rounding and
@@ -105,7 +113,7 @@ def test_amg_bicgstab_counts():
 
 def test_amg_run_parity():
     p = make_config("hetero", shape=(32, 28, 16), seed=12)
-    ov = dict(AMG, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    ov = dict(AMG, sim_type=0, inc_fact=1.0, ini_step=600.0)
     from msg123_b200.solver import GpuSolver
     g, o = GpuSolver(p, **ov), Oracle(p, **ov)
     g.init_state(); o.init_state()
@@ -133,7 +141,7 @@ def test_dense_inverse_bitexact(n, seed):
 def test_amg_lagged_setup_parity():
     """amg_lag = 1 (hierarchy of the first Newton iteration kept for the time step)."""
     p = make_config("hetero", shape=(32, 28, 16), seed=13)
-    ov = dict(AMG, amg_lag=1, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    ov = dict(AMG, amg_lag=1, sim_type=0, inc_fact=1.0, ini_step=600.0)
     from msg123_b200.solver import GpuSolver
     g, o = GpuSolver(p, **ov), Oracle(p, **ov)
     g.init_state(); o.init_state()
@@ -147,7 +155,7 @@ def test_amg_lagged_setup_parity():
 def test_amg_lag_over_steps_parity():
     """amg_lag = 3: one hierarchy serves three time steps; same rule in the oracle."""
     p = make_config("hetero", shape=(32, 28, 16), seed=14)
-    ov = dict(AMG, amg_lag=3, sim_type=0, inc_fact=1.0, ini_step=1800.0)
+    ov = dict(AMG, amg_lag=3, sim_type=0, inc_fact=1.0, ini_step=600.0)
     from msg123_b200.solver import GpuSolver
     g, o = GpuSolver(p, **ov), Oracle(p, **ov)
     g.init_state(); o.init_state()
@@ -164,7 +172,7 @@ def test_jv_mode_run_parity():
     GPU and oracle implement it alike, so the runs match as the FP64 AMG runs do, and they
     land within 1e-8 of the jv_mode = 0 run (the slope changes the line search only)."""
     p = make_config("hetero", shape=(32, 28, 16), seed=12)
-    ov = dict(AMG, sim_type=0, inc_fact=1.0, ini_step=1800.0, amg_lag=1, jv_mode=1)
+    ov = dict(AMG, sim_type=0, inc_fact=1.0, ini_step=600.0, amg_lag=1, jv_mode=1)
     from msg123_b200.solver import GpuSolver
     g, o = GpuSolver(p, **ov), Oracle(p, **ov)
     g.init_state(); o.init_state()
