@@ -80,7 +80,7 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
   if (c->timing) cudaEventRecord(c->ev[7], c->stream);
   int rc = launch_calc_func(c, h, F, true);
   if (rc) return rc;
-  *l2 = sum_part(c, nblk(c->N), &rc);   // synchronises the stream
+  *l2 = sum_part(c, flux_parts(c), &rc);   // synchronises the stream
   c->l2_last = *l2;
   if (c->timing) {
     cudaEventRecord(c->ev[0], c->stream);
@@ -99,7 +99,7 @@ static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse) {
   if (c->timing) cudaEventRecord(ev[0], c->stream);
   int rc = launch_make_matvec(c, reuse);
   if (rc) return rc;
-  double s = sum_part(c, nblk(c->N), &rc);
+  double s = sum_part(c, flux_parts(c), &rc);
   if (rc) return rc;
   if (l2_rhs) *l2_rhs = s;
   if (c->timing) cudaEventRecord(ev[1], c->stream);
@@ -593,6 +593,9 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
     ALLOC(c->lu_f, 6 * N * 4);
   }
   size_t npart = std::max((size_t)kRedBlocks * 8, 2 * (size_t)nblk((int)N) + 64);
+  // the flux passes' 3D grid can have more blocks than nblk(N) when nx or ny is not a
+  // multiple of the tile (32 x 8)
+  npart = std::max(npart, (size_t)((g->nx + 31) / 32) * ((g->ny + 7) / 8) * g->nz + 64);
   ALLOC(c->part, npart * 8);
   ALLOC(c->dres, 16 * 8);
   MSG_CUDA(cudaMallocHost((void **)&c->hpin, (size_t)kRedBlocks * 8 * 8));

@@ -109,6 +109,7 @@ int launch_velocity(msg_ctx *c, double *facev, double *pointv);
 int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
                      double *riv, double *lak, double *drn);
 int launch_wells(msg_ctx *c);
+int flux_parts(const msg_ctx *c);   // F^2 partials the flux passes write (one per block)
 
 // ---- msg_linear.cu ----------------------------------------------------------------------------
 int build_wavefront(msg_ctx *c);

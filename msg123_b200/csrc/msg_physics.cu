@@ -328,15 +328,17 @@ __device__ __forceinline__ double stage_term(const double *st, int S, int s, dou
   return __dmul_rn(__dmul_rn(__dmul_rn(hydf, abyd), delh), kri);
 }
 
+// The flux passes run on a 3D grid of 256-thread blocks, each a 32 (x) by 8 (y) tile of one
+// layer (blockIdx.z), so a cell's grid coordinates come from its block and lane with no
+// integer division; flux_parts(c) is the number of blocks (one F^2 partial each).
 template <bool ASM>
 __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
   const Geo g = a.g;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = blockIdx.x * 32 + (threadIdx.x & 31), iy = blockIdx.y * 8 + (threadIdx.x >> 5), iz = blockIdx.z;
   double f2 = 0.0;
-  if (i < g.N) {
+  if (ix < g.nx && iy < g.ny) {
     const size_t N = g.N;
-    int ix, iy, iz;
-    cell_ijk(g, i, ix, iy, iz);
+    const int i = ix + g.nx * (iy + g.ny * iz);
     const double hi = a.h[i], kri = a.kr[i];
     const double krpi = ASM ? a.kr_per[i] : 0.0;
     const int nbd[6] = {-g.nxy, -g.nx, -1, 1, g.nx, g.nxy};
@@ -427,7 +429,7 @@ __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
   }
   if (a.part) {
     double s = block_sum<256>(f2, sh);
-    if (threadIdx.x == 0) a.part[blockIdx.x] = s;
+    if (threadIdx.x == 0) a.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
   }
 }
 
@@ -629,6 +631,11 @@ __global__ void k_wells(int nwell, const int *__restrict__ w_index, const int *_
 // Host wrappers
 // ---------------------------------------------------------------------------------
 static Geo geo(const msg_ctx *c) { return Geo{c->nx, c->ny, c->nz, c->nxy, c->N}; }
+static dim3 flux_grid(const msg_ctx *c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
+int flux_parts(const msg_ctx *c) {
+  const dim3 g = flux_grid(c);
+  return (int)(g.x * g.y * g.z);
+}
 static int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
 int build_connectivity(msg_ctx *c, const msg_grid_t *g) {
@@ -744,7 +751,7 @@ int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
   FluxArgs a = flux_args(c, h);
   a.F = F;
   a.part = norm ? c->part : nullptr;
-  k_flux_res<<<nblk(c->N), 256, 0, c->stream>>>(a);
+  k_flux_res<<<flux_grid(c), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
@@ -762,7 +769,7 @@ int launch_make_matvec(msg_ctx *c, bool reuse) {
   a.dmat_f = c->dmat_f;
   a.lu_f = c->lu_f;
   a.part = c->part;
-  k_flux_asm<<<nblk(c->N), 256, 0, c->stream>>>(a);
+  k_flux_asm<<<flux_grid(c), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
