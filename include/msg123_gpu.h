@@ -89,7 +89,10 @@ typedef struct msg_params {
   int32_t guess_mode;        /* Newton initial guess: 0 = previous head (reference), 1 = linear
                                 extrapolation, 2 = learned increment                                  */
   int32_t guess_select;      /* guess_mode 2: 1 = start from whichever of the learned and the
-                                extrapolated guess has the smaller ||F|| (two residual evaluations);
+                                extrapolated guess has the smaller ||F|| (two residual evaluations;
+                                when the extrapolation wins, the first assembly reuses its van
+                                Genuchten state); 2 = as 1, and after the extrapolation wins the
+                                network pauses for 1, 2, 4, then 8 steps (reset when it wins);
                                 a failed solve from the learned guess is redone from the
                                 extrapolation when the guess was not vetted (0) or Newton broke
                                 down (NaN, divergence), else the step is rejected as usual          */

@@ -80,7 +80,7 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
   if (c->timing) cudaEventRecord(c->ev[7], c->stream);
   int rc = launch_calc_func(c, h, F, true);
   if (rc) return rc;
-  *l2 = sum_part(c, flux_parts(c), &rc);   // synchronises the stream
+  *l2 = sum_part(c, res_parts(c), &rc);   // synchronises the stream
   c->l2_last = *l2;
   if (c->timing) {
     cudaEventRecord(c->ev[0], c->stream);
@@ -352,7 +352,10 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     // from the second iteration on, the previous iteration ended with F evaluated at
     // head_new (line search or the closing evaluation), leaving S, kr and the storage
     // term there in srat_new / kr / sto
-    if ((rc = make_matvec(c, &l2r, c->out_iter > 1))) return rc;
+    // the first assembly reuses S, kr and the storage term when the guess selection left
+    // them at head_new (the chosen guess was the last one evaluated)
+    if ((rc = make_matvec(c, &l2r, c->out_iter > 1 || c->vg_at_head))) return rc;
+    c->vg_at_head = 0;
     if ((rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
     if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }
     if ((rc = copy_d2d(c, c->head_pre, c->head_new, n))) return rc;
@@ -460,7 +463,10 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
     }
     msg_stats_t st;
     bool learned_try = false;
-    if (c->prm.guess_mode == 2 && c->timestep_num > 0 && conv != 0 && learned_ready(c)) {
+    c->vg_at_head = 0;
+    const bool paused = c->prm.guess_select == 2 && c->guess_skip > 0;
+    if (paused) c->guess_skip--;
+    if (c->prm.guess_mode == 2 && c->timestep_num > 0 && conv != 0 && learned_ready(c) && !paused) {
       if ((rc = learned_guess(c))) return rc;       // head_new <- h_old + CNN increment
       learned_try = true;
       if (c->prm.guess_select) {
@@ -471,9 +477,17 @@ static int advance(msg_ctx *c, int nsteps, double rech_until, double rech_after,
         MSG_CHECK_LAUNCH();
         if ((rc = func_norm(c, c->head_pre, c->new_f, &fe))) return rc;
         if (!(fl < fe)) {
+          // the extrapolation was evaluated last: its S, kr and storage serve the first assembly
           if ((rc = copy_d2d(c, c->head_new, c->head_pre, n))) return rc;
           learned_try = false;
           c->guess_rejected++;
+          c->vg_at_head = 1;
+          if (c->prm.guess_select == 2) {   // back off: 1, 2, 4, 8 steps without the network
+            c->guess_backoff = std::min(std::max(2 * c->guess_backoff, 1), 8);
+            c->guess_skip = c->guess_backoff;
+          }
+        } else {
+          c->guess_backoff = 0;
         }
       }
     } else if (c->prm.guess_mode >= 1 && c->timestep_num > 0) {
@@ -617,6 +631,7 @@ int msg_gpu_create(const msg_grid_t *grid, const msg_params_t *params, msg_ctx_t
   if (params->vg_form != 0 && params->vg_form != 1) { set_error("vg_form must be 0 or 1"); return MSG_ERR_ARG; }
   if (params->precision != 0 && params->precision != 1) { set_error("precision must be 0 or 1"); return MSG_ERR_ARG; }
   if (params->jv_mode != 0 && params->jv_mode != 1) { set_error("jv_mode must be 0 or 1"); return MSG_ERR_ARG; }
+  if (params->guess_select < 0 || params->guess_select > 2) { set_error("guess_select must be 0, 1 or 2"); return MSG_ERR_ARG; }
   const void *req[] = {grid->reta, grid->retn, grid->resi, grid->poro, grid->ss, grid->ksx, grid->ksy, grid->ksz,
                        grid->cell_top, grid->cell_vol, grid->dis2face, grid->face_area, grid->surf_top, grid->surf_bott};
   for (auto q : req) if (!q) { set_error("required grid array is NULL"); return MSG_ERR_ARG; }

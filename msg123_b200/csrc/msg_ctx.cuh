@@ -77,6 +77,8 @@ struct msg_ctx {
   int timestep_num, last_conv, last_out;
   int guess_fallbacks;                           // learned guesses replaced by extrapolation
   int guess_rejected;                            // learned guesses not used (larger residual)
+  int guess_skip, guess_backoff;                 // guess_select 2: steps left without the network, next pause
+  int vg_at_head;                                // S, kr, storage in memory are those of head_new (reuse)
   // convergence log (msg_gpu_set_convlog): records of the Newton iterations, oldest first
   void *clog;                                    // std::deque<msg_convrec_t> (msg_api.cu)
   int clog_on;
@@ -109,7 +111,8 @@ int launch_velocity(msg_ctx *c, double *facev, double *pointv);
 int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *wel, double *rec, double *sur,
                      double *riv, double *lak, double *drn);
 int launch_wells(msg_ctx *c);
-int flux_parts(const msg_ctx *c);   // F^2 partials the flux passes write (one per block)
+int flux_parts(const msg_ctx *c);   // F^2 partials the assembly pass writes (one per block)
+int res_parts(const msg_ctx *c);    // F^2 partials the residual pass writes (one per block)
 
 // ---- msg_linear.cu ----------------------------------------------------------------------------
 int build_wavefront(msg_ctx *c);
