@@ -80,7 +80,7 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
   if (c->timing) cudaEventRecord(c->ev[7], c->stream);
   int rc = launch_calc_func(c, h, F, true);
   if (rc) return rc;
-  *l2 = sum_part(c, res_parts(c), &rc);   // synchronises the stream
+  *l2 = sum_part(c, flux_parts(c), &rc);   // synchronises the stream
   c->l2_last = *l2;
   if (c->timing) {
     cudaEventRecord(c->ev[0], c->stream);

@@ -112,7 +112,6 @@ int launch_cell_mass(msg_ctx *c, double *sto, double *con, double *sea, double *
                      double *riv, double *lak, double *drn);
 int launch_wells(msg_ctx *c);
 int flux_parts(const msg_ctx *c);   // F^2 partials the assembly pass writes (one per block)
-int res_parts(const msg_ctx *c);    // F^2 partials the residual pass writes (one per block)
 
 // ---- msg_linear.cu ----------------------------------------------------------------------------
 int build_wavefront(msg_ctx *c);

@@ -433,111 +433,6 @@ __device__ __forceinline__ void flux_body(const FluxArgs &a, double *sh) {
   }
 }
 
-// calc_func in one pass (k_cell<false> + k_flux_res fused): a block owns a 32 x 8 column
-// tile and marches down `zc` layers.  For each layer it evaluates van Genuchten / Mualem for
-// its own cells (writing S, kr and the storage term as k_cell does) and for the 80 cells
-// of the tile's x-y halo (kr and h only, into shared memory); the up and down neighbours
-// come from the same thread's previous and next layer, held in registers.  Then each cell
-// forms F exactly as flux_body<false> does.  The FP64-bound vG work and the flux pass's
-// load latency overlap inside one kernel, at the price of 80 halo evaluations per 256
-// cells.  One F^2 partial per block (each thread sums its layers first).
-template <int FORM>
-__global__ void __launch_bounds__(256) k_res_fused(CellArgs ca, FluxArgs a, int zc) {
-  __shared__ double sh_h[10][34], sh_k[10][34];
-  __shared__ double sh_red[8];
-  const Geo g = a.g;
-  const size_t N = g.N;
-  const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
-  const int ix = x0 + tx, iy = y0 + ty;
-  const bool live = ix < g.nx && iy < g.ny;
-  const int z0 = blockIdx.z * zc, z1 = min(z0 + zc, g.nz);
-  // halo slot of threads 0..79: rows y0-1 and y0+8 (32 each), columns x0-1 and x0+32 (8 each)
-  int hx = -1, hy = -1, hr = 0, hc = 0;
-  if (t < 32) { hx = x0 + t; hy = y0 - 1; hr = 0; hc = t + 1; }
-  else if (t < 64) { hx = x0 + t - 32; hy = y0 + 8; hr = 9; hc = t - 31; }
-  else if (t < 72) { hx = x0 - 1; hy = y0 + t - 64; hr = t - 63; hc = 0; }
-  else if (t < 80) { hx = x0 + 32; hy = y0 + t - 72; hr = t - 71; hc = 33; }
-  const bool hlive = t < 80 && hx >= 0 && hx < g.nx && hy >= 0 && hy < g.ny;
-  const int col = ix + g.nx * iy, hcol = hx + g.nx * hy;
-  auto own = [&](int z, double &h, double &kr, double &S, double &sto) {
-    const int i = col + g.nxy * z;
-    h = ca.h[i];
-    VG v = vg_eval<FORM>(h, ca.top[i], 0.0, ca.reta[i], ca.retn[i], ca.resi[i], ca.poro[i], ca.ss[i]);
-    double ch1 = __dmul_rn(__dmul_rn(v.alp, ca.s_old[i]), ca.h_old[i]);
-    double ch2 = __dmul_rn(__dmul_rn(v.alp, v.S), h);
-    double ch = __dadd_rn(__dsub_rn(ch2, ch1), __dmul_rn((double)ca.poro[i], __dsub_rn(v.S, ca.s_old[i])));
-    sto = __dmul_rn(__dmul_rn(-ch, ca.delt_inv), ca.vol[i]);
-    kr = v.kr;
-    S = v.S;
-  };
-  double h_m = 0.0, k_m = 0.0, h_c = 0.0, k_c = 0.0, S_c = 0.0, sto_c = 0.0, f2 = 0.0;
-  if (live) {
-    own(z0, h_c, k_c, S_c, sto_c);
-    if (z0 > 0) { double s_, t_; own(z0 - 1, h_m, k_m, s_, t_); }
-  }
-  for (int z = z0; z < z1; ++z) {
-    double h_p = 0.0, k_p = 0.0, S_p = 0.0, sto_p = 0.0;
-    if (live && z + 1 < g.nz) own(z + 1, h_p, k_p, S_p, sto_p);
-    if (hlive) {
-      const int j = hcol + g.nxy * z;
-      const double hj = ca.h[j];
-      sh_h[hr][hc] = hj;
-      sh_k[hr][hc] = vg_eval<FORM>(hj, ca.top[j], 0.0, ca.reta[j], ca.retn[j], ca.resi[j], ca.poro[j], ca.ss[j]).kr;
-    }
-    sh_h[ty + 1][tx + 1] = h_c;
-    sh_k[ty + 1][tx + 1] = k_c;
-    __syncthreads();
-    if (live) {
-      const int i = col + g.nxy * z;
-      ca.srat[i] = S_c; ca.kr[i] = k_c; ca.sto[i] = sto_c;
-      const double hi = h_c, kri = k_c;
-      const bool has[6] = {z > 0, iy > 0, ix > 0, ix < g.nx - 1, iy < g.ny - 1, z < g.nz - 1};
-      const double hn[6] = {h_m, sh_h[ty][tx + 1], sh_h[ty + 1][tx], sh_h[ty + 1][tx + 2], sh_h[ty + 2][tx + 1], h_p};
-      const double kn[6] = {k_m, sh_k[ty][tx + 1], sh_k[ty + 1][tx], sh_k[ty + 1][tx + 2], sh_k[ty + 2][tx + 1], k_p};
-      const int nbd[6] = {-g.nxy, -g.nx, -1, 1, g.nx, g.nxy};
-      double cf = 0.0;
-#pragma unroll
-      for (int d = 0; d < 6; ++d) {
-        if (has[d]) {
-          const int j = i + nbd[d];
-          const size_t fi = (d < 3) ? (size_t)d * N + i : (size_t)(5 - d) * N + j;
-          const double delhead = __dsub_rn(hn[d], hi);
-          const double relat = upwind(-delhead, kri, kn[d]);
-          cf = __dadd_rn(cf, __dmul_rn(__dmul_rn(__dmul_rn(a.hy[fi], relat), a.ab[fi]), delhead));
-        }
-      }
-      double fs = 0.0, sea = 0.0;
-      if (z == 0) {
-        const int s = i;
-        double delh, over, dmy;
-        double sf = surf_term(hi, a.surf_head[s], a.surf_top[s], a.surf_bott[s], a.surf_reli[s], a.surf_parm[s],
-                              a.hydf_surf[s], a.abyd_surf[s], kri, delh, over);
-        double rv = 0.0, lk = 0.0;
-        if (a.riv) rv = stage_term(a.riv, g.nxy, s, hi, a.hydf_surf[s], kri, 0.0, a.newper_inv, false, dmy);
-        if (a.lak) lk = stage_term(a.lak, g.nxy, s, hi, a.hydf_surf[s], kri, 0.0, a.newper_inv, false, dmy);
-        fs = __dadd_rn(__dadd_rn(__dadd_rn(a.calc_rech[s], sf), rv), lk);
-        if (a.sea_top)
-          sea = __dmul_rn(__dmul_rn(__dmul_rn(a.sea_hydf[s], kri), a.sea_abyd[s]), __dsub_rn(a.read_seal[s], hi));
-      }
-      const double wel = a.calc_well ? a.calc_well[i] : 0.0;
-      double f = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(fs, sto_c), cf), wel), sea);
-      if (a.free_drainage && z == g.nz - 1) {
-        const double coef = a.drain[i - (g.nz - 1) * g.nxy];
-        if (coef != 0.0) f = __dadd_rn(f, -__dmul_rn(coef, kri));
-      }
-      a.F[i] = f;
-      f2 = __dadd_rn(f2, __dmul_rn(f, f));
-    }
-    __syncthreads();
-    h_m = h_c; k_m = k_c; h_c = h_p; k_c = k_p; S_c = S_p; sto_c = sto_p;
-  }
-  if (a.part) {
-    double s = block_sum<256>(f2, sh_red);
-    if (t == 0) a.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
-  }
-}
-
 // Residual pass: at most 48 registers so that five 256-thread blocks stay resident per SM
 // (the pass is bound by the latency of its 27 loads per cell, not by bandwidth).
 __global__ void __launch_bounds__(256, 5) k_flux_res(FluxArgs a) {
@@ -848,26 +743,15 @@ static CellArgs cell_args(msg_ctx *c, const double *h) {
   return a;
 }
 
-// Layers per block of the fused residual pass: the grid has ceil(nx/32) x ceil(ny/8) x
-// ceil(nz/zc) blocks; each block evaluates two layers beyond its own (the neighbours above
-// and below its slab), so zc trades that overhead against the number of blocks.
-static int res_zc(const msg_ctx *c) { return std::min(c->nz, 24); }
-static dim3 res_grid(const msg_ctx *c) {
-  const int zc = res_zc(c);
-  return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, (c->nz + zc - 1) / zc);
-}
-int res_parts(const msg_ctx *c) {
-  const dim3 g = res_grid(c);
-  return (int)(g.x * g.y * g.z);
-}
-
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
-  CellArgs ca = cell_args(c, h);
+  const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
+  auto k = c->prm.vg_form ? k_cell<false, false, 1> : k_cell<false, false, 0>;
+  k<<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, h));
+  MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, h);
   a.F = F;
   a.part = norm ? c->part : nullptr;
-  auto k = c->prm.vg_form ? k_res_fused<1> : k_res_fused<0>;
-  k<<<res_grid(c), 256, 0, c->stream>>>(ca, a, res_zc(c));
+  k_flux_res<<<flux_grid(c), 256, 0, c->stream>>>(a);
   MSG_CHECK_LAUNCH();
   return MSG_OK;
 }
