@@ -78,6 +78,7 @@ typedef struct orc {
   double errtol, bnorm, rnorm;
   /* AMG */
   int nlevel;
+  int aggr_mode;             /* 0: MIS-2 (the CUDA library's), 1: make_aggregation's heap */
   orc_level lev[16];
   double *slope_rhs;         /* vector the line-search slope reads (Q2) */
   double *lin_r;             /* BiCGStab's last residual rhs - A x (jv_mode = 1) */
@@ -786,6 +787,125 @@ static int accumulate_sorted(const int *pc, const double *pv, int m, int *oc, do
   return u;
 }
 
+/* ---------------------------------------------------------------------------------
+ * The reference's aggregation, make_aggregation with its priority queue
+ * (Make_amg_matrix.f90:113-222) and remove_enter_quedeep / remove_que / enter_que
+ * (:633-768), on the strength graph of make_grapfilt (:67-111).  It serves as a
+ * structural known answer next to the MIS-2 above: the CUDA library does not run it.
+ *
+ * The queue is a binary max-heap on positions 1..qsize keyed by a priority (qflag),
+ * initially every node with at least one strong connection, priority 1, in index order.
+ * Removing a node moves the larger child up into the hole until the hole reaches a node
+ * whose children are holes or absent (no re-heaping from the end: holes stay in the
+ * array, and the queue is empty when position 1 is a hole).  Each round takes the node
+ * at the top as a new root: the root and its strong neighbours form the aggregate, the
+ * distance-2 nodes leave the queue unaggregated, and each distance-3 node still queued
+ * gains one priority and moves up.  Finally the first node in index order with an
+ * aggregated strong neighbour adopts that neighbour's aggregate and the scan stops (the
+ * `exit aggre_check` of :169-182, which leaves every other distance-2 node out of the
+ * aggregates).  Nodes are 0-based here; gnum stores node + 1 so that 0 means unmarked.
+ * --------------------------------------------------------------------------------- */
+typedef struct heapq {
+  int qsize;
+  int *qflag, *q2g, *pos;    /* priority and node per position; position per node (0: out) */
+} heapq;
+
+static void heap_remove(heapq *h, int node) {          /* remove_que (:684-727) */
+  int qnum = h->pos[node];
+  h->qflag[qnum] = 0;
+  h->q2g[qnum] = -1;
+  int temq = 2 * qnum;
+  while (temq <= h->qsize) {
+    if (temq + 1 <= h->qsize && h->qflag[temq + 1] > h->qflag[temq]) temq++;
+    if (h->qflag[temq] == 0) break;
+    int temg = h->q2g[temq];
+    h->qflag[qnum] = h->qflag[temq];
+    h->q2g[qnum] = temg;
+    h->pos[temg] = qnum;
+    h->qflag[temq] = 0;
+    h->q2g[temq] = -1;
+    qnum = temq;
+    temq = 2 * qnum;
+  }
+}
+
+static void heap_raise(heapq *h, int node) {           /* enter_que (:729-766) */
+  int qnum = h->pos[node], temq = qnum / 2;
+  while (qnum > 1 && h->qflag[temq] < h->qflag[qnum]) {
+    int tf = h->qflag[temq]; h->qflag[temq] = h->qflag[qnum]; h->qflag[qnum] = tf;
+    int g1 = h->q2g[qnum], g2 = h->q2g[temq];
+    h->q2g[temq] = g1; h->q2g[qnum] = g2;
+    h->pos[g2] = qnum; h->pos[g1] = temq;
+    qnum = temq;
+    temq = qnum / 2;
+  }
+}
+
+/* agg[i]: aggregate of node i (0-based) or -1; returns the number of aggregates.
+ * sidx / slu / offrow: the strength graph (CSR positions of the strong entries of row i in
+ * slu[sidx[i]..sidx[i+1]), their columns offrow[slu[.]]). */
+static int heap_aggregate(int n, const int *sidx, const int *slu, const int *offrow, int *agg) {
+  heapq h;
+  h.qflag = xc(n + 2, sizeof(int)); h.q2g = xc(n + 2, sizeof(int)); h.pos = xc(n, sizeof(int));
+  int *gnum = xc(n, sizeof(int)), *lay2 = xc(n, sizeof(int));
+  int *num = xc(n, sizeof(int));               /* aggr_num: 1-based aggregate, 0 = none */
+  h.qsize = 0;
+  for (int i = 0; i < n; ++i) {
+    if (sidx[i + 1] > sidx[i]) { h.qsize++; h.pos[i] = h.qsize; h.qflag[h.qsize] = 1; h.q2g[h.qsize] = i; }
+  }
+  int nc = 0;
+  while (h.qsize > 0 && h.qflag[1] != 0) {
+    const int i = h.q2g[1];
+    nc++;
+    num[i] = nc;
+    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+      const int j = offrow[slu[s]];
+      num[j] = nc;
+      if (h.pos[j] > 0) heap_remove(&h, j);
+      h.pos[j] = 0;
+      gnum[j] = i + 1;
+    }
+    heap_remove(&h, i);
+    h.pos[i] = 0;
+    gnum[i] = i + 1;
+    /* remove_enter_quedeep (:633-682) */
+    int nl2 = 0;
+    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+      const int j = offrow[slu[s]];
+      for (int t = sidx[j]; t < sidx[j + 1]; ++t) {
+        const int l2 = offrow[slu[t]];
+        if (gnum[l2] != i + 1) {
+          gnum[l2] = i + 1;
+          lay2[nl2++] = l2;
+          if (h.pos[l2] > 0) { heap_remove(&h, l2); h.pos[l2] = 0; }
+        }
+      }
+    }
+    for (int k = 0; k < nl2; ++k) {
+      const int j = lay2[k];
+      for (int t = sidx[j]; t < sidx[j + 1]; ++t) {
+        const int l3 = offrow[slu[t]];
+        if (gnum[l3] != i + 1) {
+          gnum[l3] = i + 1;
+          if (h.pos[l3] > 0) { h.qflag[h.pos[l3]]++; heap_raise(&h, l3); }
+        }
+      }
+    }
+  }
+  /* aggre_check (:169-182): every node is out of the queue now */
+  for (int i = 0; i < n; ++i) {
+    int done = 0;
+    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+      const int j = offrow[slu[s]];
+      if (num[j] > 0) { num[i] = num[j]; done = 1; break; }
+    }
+    if (done) break;
+  }
+  for (int i = 0; i < n; ++i) agg[i] = num[i] - 1;
+  free(h.qflag); free(h.q2g); free(h.pos); free(gnum); free(lay2); free(num);
+  return nc;
+}
+
 /* Export for tests: aggregation of the last setup. */
 static int *g_last_agg[16];
 
@@ -810,57 +930,62 @@ static int own_coarsen(orc_t *o, int lv) {
     tdm[i] = t;
     sidx[i + 1] = ns;
   }
-  /* MIS-2 on the directed strength graph */
-  uint64_t *st = xc(n, sizeof(uint64_t)), *t0 = xc(n, sizeof(uint64_t));
-  uint64_t *t1 = xc(n, sizeof(uint64_t)), *t2 = xc(n, sizeof(uint64_t));
-  for (int i = 0; i < n; ++i) st[i] = (sidx[i + 1] > sidx[i]) ? MIS_UNDEC : 0;
-  for (int round = 0; round < 64; ++round) {
-    int undec = 0;
-    for (int i = 0; i < n; ++i) { t0[i] = mis_tuple(st[i], i, lv); if (st[i] == MIS_UNDEC) undec++; }
-    if (!undec) break;
-    for (int i = 0; i < n; ++i) {
-      uint64_t m = t0[i];
-      for (int s = sidx[i]; s < sidx[i + 1]; ++s) { uint64_t v = t0[F->offrow[slu[s]]]; if (v > m) m = v; }
-      t1[i] = m;
-    }
-    for (int i = 0; i < n; ++i) {
-      uint64_t m = t1[i];
-      for (int s = sidx[i]; s < sidx[i + 1]; ++s) { uint64_t v = t1[F->offrow[slu[s]]]; if (v > m) m = v; }
-      t2[i] = m;
-    }
-    for (int i = 0; i < n; ++i) {
-      if (st[i] != MIS_UNDEC) continue;
-      if ((uint32_t)(t2[i] & 0xffffffffu) == (uint32_t)i) st[i] = MIS_ROOT;
-      else if ((t2[i] >> 62) == MIS_ROOT) st[i] = 0;   /* decided non-root: drops out of the max */
-    }
-  }
-  /* aggregate numbering: roots in index order */
-  int *agg = xc(n, sizeof(int)), *agg2 = xc(n, sizeof(int));
+  int *agg = xc(n, sizeof(int));
   int nc = 0;
-  for (int i = 0; i < n; ++i) agg[i] = (st[i] == MIS_ROOT) ? nc++ : -1;
-  /* pass A: non-roots join the best root among their strong neighbours */
-  for (int i = 0; i < n; ++i) {
-    agg2[i] = agg[i];
-    if (agg[i] >= 0) continue;
-    uint64_t best = 0; int bj = -1;
-    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
-      int j = F->offrow[slu[s]];
-      if (st[j] == MIS_ROOT) { uint64_t v = mis_tuple(MIS_UNDEC, j, lv); if (v > best) { best = v; bj = j; } }
+  if (o->aggr_mode == 1) {
+    nc = heap_aggregate(n, sidx, slu, F->offrow, agg);
+  } else {
+    /* MIS-2 on the directed strength graph */
+    uint64_t *st = xc(n, sizeof(uint64_t)), *t0 = xc(n, sizeof(uint64_t));
+    uint64_t *t1 = xc(n, sizeof(uint64_t)), *t2 = xc(n, sizeof(uint64_t));
+    for (int i = 0; i < n; ++i) st[i] = (sidx[i + 1] > sidx[i]) ? MIS_UNDEC : 0;
+    for (int round = 0; round < 64; ++round) {
+      int undec = 0;
+      for (int i = 0; i < n; ++i) { t0[i] = mis_tuple(st[i], i, lv); if (st[i] == MIS_UNDEC) undec++; }
+      if (!undec) break;
+      for (int i = 0; i < n; ++i) {
+        uint64_t m = t0[i];
+        for (int s = sidx[i]; s < sidx[i + 1]; ++s) { uint64_t v = t0[F->offrow[slu[s]]]; if (v > m) m = v; }
+        t1[i] = m;
+      }
+      for (int i = 0; i < n; ++i) {
+        uint64_t m = t1[i];
+        for (int s = sidx[i]; s < sidx[i + 1]; ++s) { uint64_t v = t1[F->offrow[slu[s]]]; if (v > m) m = v; }
+        t2[i] = m;
+      }
+      for (int i = 0; i < n; ++i) {
+        if (st[i] != MIS_UNDEC) continue;
+        if ((uint32_t)(t2[i] & 0xffffffffu) == (uint32_t)i) st[i] = MIS_ROOT;
+        else if ((t2[i] >> 62) == MIS_ROOT) st[i] = 0;   /* decided non-root: drops out of the max */
+      }
     }
-    if (bj >= 0) agg2[i] = agg[bj];
-  }
-  /* pass B: the rest join the best already-assigned strong neighbour */
-  for (int i = 0; i < n; ++i) {
-    agg[i] = agg2[i];
-    if (agg2[i] >= 0) continue;
-    uint64_t best = 0; int bj = -1;
-    for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
-      int j = F->offrow[slu[s]];
-      if (agg2[j] >= 0) { uint64_t v = mis_tuple(MIS_UNDEC, j, lv); if (v > best) { best = v; bj = j; } }
+    /* aggregate numbering: roots in index order */
+    int *agg2 = xc(n, sizeof(int));
+    for (int i = 0; i < n; ++i) agg[i] = (st[i] == MIS_ROOT) ? nc++ : -1;
+    /* pass A: non-roots join the best root among their strong neighbours */
+    for (int i = 0; i < n; ++i) {
+      agg2[i] = agg[i];
+      if (agg[i] >= 0) continue;
+      uint64_t best = 0; int bj = -1;
+      for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+        int j = F->offrow[slu[s]];
+        if (st[j] == MIS_ROOT) { uint64_t v = mis_tuple(MIS_UNDEC, j, lv); if (v > best) { best = v; bj = j; } }
+      }
+      if (bj >= 0) agg2[i] = agg[bj];
     }
-    if (bj >= 0) agg[i] = agg2[bj];
+    /* pass B: the rest join the best already-assigned strong neighbour */
+    for (int i = 0; i < n; ++i) {
+      agg[i] = agg2[i];
+      if (agg2[i] >= 0) continue;
+      uint64_t best = 0; int bj = -1;
+      for (int s = sidx[i]; s < sidx[i + 1]; ++s) {
+        int j = F->offrow[slu[s]];
+        if (agg2[j] >= 0) { uint64_t v = mis_tuple(MIS_UNDEC, j, lv); if (v > best) { best = v; bj = j; } }
+      }
+      if (bj >= 0) agg[i] = agg2[bj];
+    }
+    free(agg2); free(st); free(t0); free(t1); free(t2);
   }
-  free(agg2); free(st); free(t0); free(t1); free(t2);
   free(g_last_agg[lv]); g_last_agg[lv] = agg;
   if (nc == 0 || nc >= n) { free(sidx); free(slu); free(tdm); return 0; }
   /* rows of P longer than P_ROW_MAX stop the coarsening (the GPU keeps them in registers) */
@@ -1682,6 +1807,8 @@ void orc_vecjacf(void *h, const double *x, const double *v, double *out) { calc_
 
 /* AMG inspection for structural tests */
 int orc_amg_nlevel(void *h) { return ((orc_t *)h)->nlevel; }
+/* Aggregation of the own AMG's next setups: 0 MIS-2, 1 make_aggregation's heap. */
+void orc_set_aggregation(void *h, int mode) { ((orc_t *)h)->aggr_mode = mode; }
 void orc_amg_level_sizes(void *h, int lv, int *n, int *nnz, int *pnnz) {
   orc_t *o = h; orc_level *L = &o->lev[lv];
   *n = L->n; *nnz = L->nnz; *pnnz = (lv > 0 && L->pindex) ? L->pindex[o->lev[lv - 1].n] : 0;

@@ -55,6 +55,7 @@ def lib():
         L.orc_velocity.argtypes = [vp, abi.PD, abi.PD]
         L.orc_amg_level_sizes.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PI]
         L.orc_amg_level.argtypes = [vp, C.c_int, abi.PI, abi.PI, abi.PD, abi.PD, abi.PI, abi.PI, abi.PD, abi.PI]
+        L.orc_set_aggregation.argtypes = [vp, C.c_int]
         _lib = L
     return _lib
 
@@ -239,6 +240,12 @@ class Oracle:
         return {k: lib().orc_counter(C.c_void_p(self.h), i) for i, k in enumerate(("func", "matvec", "prec"))}
 
     # -- AMG inspection ---------------------------------------------------------------
+    def set_aggregation(self, mode):
+        """Aggregation of the next AMG setups (precon_type 1, ref_quirks 0): 0 the MIS-2 the
+        CUDA library runs, 1 the priority-queue aggregation of make_aggregation
+        (Make_amg_matrix.f90:113-222, :633-768), a structural comparison only."""
+        lib().orc_set_aggregation(C.c_void_p(self.h), int(mode))
+
     def amg_levels(self):
         L = lib()
         nl = L.orc_amg_nlevel(C.c_void_p(self.h))
