@@ -787,6 +787,27 @@ __global__ void k_b2f(int n, const double *b, float *bf) {
 // products of a lane are added in entry order.  Every lane reaches the shuffles.
 __device__ __forceinline__ float ldf(const float *p) { return *p; }
 __device__ __forceinline__ float ldf(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+// Sequential sum of one CSR row of float weights against a gathered vector, loads issued
+// four entries at a time (same order of additions as the plain loop).
+__device__ __forceinline__ float csr_row_f4(int beg, int end, const int *cl, const float *val, const float *x) {
+  float s = 0.f;
+  for (int k = beg; k < end; k += 4) {
+    int c[4];
+    float a[4], xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int kk = k + u;
+      c[u] = kk < end ? cl[kk] : -1;
+      a[u] = kk < end ? val[kk] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (c[u] >= 0) s += a[u] * xv[u];
+  }
+  return s;
+}
 // Two rows per quad: the quad walks rows 2Q and 2Q+1 together (column and value loads of
 // both rows, then the gathers of both), so a warp keeps sixteen rows' loads in flight
 // (4% off the mixed V-cycle at 25.2M cells against one row per quad).  Launch with
