@@ -300,6 +300,28 @@ def prep_arm(prob, kw, src, cnn, end_time=None):
     return g
 
 
+class nvtx_range:
+    """An NVTX range around a region (visible to a profiler that filters on it, e.g.
+    ncu --nvtx --nvtx-include value_window/); a no-op where no NVTX runtime is loaded."""
+
+    def __init__(self, name):
+        self.name = name
+
+    def __enter__(self):
+        try:
+            import torch
+            torch.cuda.nvtx.range_push(self.name)
+            self.ok = True
+        except Exception:
+            self.ok = False
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            import torch
+            torch.cuda.nvtx.range_pop()
+
+
 def run_arm(g, steps):
     """Advance by `steps` accepted steps (or to the context's end time): (stats, device ms,
     (learned guesses redone from the extrapolation, learned guesses not used))."""
@@ -425,7 +447,7 @@ def main():
     ga = prep_arm(prob, FAST, gw, cnn)
     barrier(dist)
     l0 = launch_count()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk, nvtx_range("value_window"):
         st, ms, fb = run_arm(ga, K)
     launches = launch_count() - l0
     value_arm = arm_stats(prob, st, ms, dist, fb)

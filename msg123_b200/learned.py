@@ -128,6 +128,10 @@ class Cnn:
     def attach(self, solver):
         _check(_lib().msg_gpu_cnn_attach(solver.h, self.h), "cnn_attach")
 
+    def detach(self, solver):
+        """The solver stops using the network (guess_mode 2 falls back to extrapolation)."""
+        _check(_lib().msg_gpu_cnn_attach(solver.h, None), "cnn_attach")
+
 
 def unpack(w):
     """Flat parameter vector -> list of (W[27,16,16] (tap, co, ci), b[16]) per layer."""
