@@ -5,7 +5,7 @@ and settings the benchmark measures, not only on small grids.
   (BiCGStab + AMG rebuilt at every Newton iteration, Newton from the previous head,
   adaptive dt from 600 s) over its first four accepted steps;
 * the value path of the benchmark (mixed precision, learned initial guess with the
-  shipped weights, AMG kept for 4 steps, two-pow kr, slope from BiCGStab's residual) on
+  shipped weights, AMG kept for 12 steps, two-pow kr, slope from BiCGStab's residual) on
   a 1,048,576-cell block of the 25.2M-cell workload's generator (sigma_lnK = 1.5) over
   twelve steps, against the FP64 oracle solved to a 1000x tighter Newton tolerance at the
   same simulated times (the time step grows by a fixed factor, so both runs meet at the
@@ -28,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 HEAD_TOL = 1e-8
 PLAIN = dict(precon_type=1, ref_quirks=0, precision=0, amg_lag=0, guess_mode=0, vg_form=0)
-VALUE = dict(precon_type=1, ref_quirks=0, precision=1, amg_lag=4, guess_mode=2, guess_select=0, vg_form=1,
+VALUE = dict(precon_type=1, ref_quirks=0, precision=1, amg_lag=12, guess_mode=2, guess_select=0, vg_form=1,
              jv_mode=1)
 
 
