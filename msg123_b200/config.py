@@ -63,6 +63,11 @@ class Problem:
     nsteps: int
     params: dict = field(default_factory=dict)
     lnk: np.ndarray = None    # ln Ks field (m/s), kept for the learned guess features
+    # the unscaled inputs in the units a reference deck holds (deck.write_deck): dx, dy, dz
+    # and z_top (m), per-cell float32 alpha (1/m), n, residual and saturated water content,
+    # Ss (1/m), Ks x/y/z (m/s), float64 initial heads (m), rain (mm/h) and its duration (h),
+    # sea head (m, ponded top)
+    phys: dict = None
 
     @property
     def ncalc(self):
@@ -168,10 +173,14 @@ def make_box(shape=(20, 20, 50), d=(0.1, 0.1, 0.1), nsteps=48, **pkw):
                          maxinn_iter=400, precon_type=0, sim_type=0, ini_step=1800.0, inc_fact=1.0,
                          end_time=1800.0 * nsteps)
     prm.update(pkw)
+    phys = dict(dx=dx, dy=dy, dz=dz, z_top=nz * dz, alpha=full(3.35), n=full(2.0), resi=full(0.102),
+                ths=full(0.368), ss=full(1.0e-5), ksx=full(9.22e-5), ksy=full(9.22e-5), ksz=full(9.22e-5),
+                head0=np.repeat(np.array([(nz - k) * dz for k in range(nz)]), nx * ny) - 10.0,
+                rain_mm_h=0.0, rain_hours=0.0, sea_head=nz * dz + 0.05)
     return Problem("box", nx, ny, nz, 1, 1, reta, full(2.0), full(0.102), full(0.368), ss,
                    ks.copy(), ks.copy(), ks.copy(), cell_top, cell_vol, dis, area,
                    np.full(nx * ny, ar), surf, surf.copy(), np.zeros(nx * ny), np.zeros(nx * ny),
-                   sea, head0, np.zeros(nx * ny), 1.0e30, 1.0, nsteps, prm)
+                   sea, head0, np.zeros(nx * ny), 1.0e30, 1.0, nsteps, prm, phys=phys)
 
 
 def make_box1r(shape=(20, 20, 50), nsteps=48, criteria=1.0e-6, **pkw):
@@ -215,11 +224,16 @@ def make_hetero(shape=(256, 256, 64), d=(1.0, 1.0, 0.25), seed=2024, sigma=1.0, 
                          maxinn_iter=100, precon_type=1, ref_quirks=0, amg_coarse_max=128, sim_type=1, ini_step=600.0,
                          max_step=3600.0, end_time=1.0e30)
     prm.update(pkw)
+    phys = dict(dx=dx, dy=dy, dz=dz, z_top=nz * dz, alpha=alpha.astype(F32), n=nvg.astype(F32),
+                resi=np.full(N, 0.05, dtype=F32), ths=ths.astype(F32), ss=np.full(N, 1.0e-5, dtype=F32),
+                ksx=np.exp(lnk).astype(F32), ksy=np.exp(lnk).astype(F32), ksz=np.exp(lnk).astype(F32),
+                head0=np.full(N, float(F32(nz * dz - wt_depth))), rain_mm_h=rain_mm_h, rain_hours=rain_hours,
+                sea_head=None)
     p = Problem("hetero", nx, ny, nz, 0, 0, reta, nvg.astype(F32), np.full(N, 0.05, dtype=F32),
                 ths.astype(F32), ss, ks.copy(), ks.copy(), ks.copy(), cell_top, cell_vol, dis, area,
                 np.full(nx * ny, ar), top_surface, top_surface.copy(), np.zeros(nx * ny),
                 np.zeros(nx * ny), np.zeros(nx * ny), head0, rech, rain_hours * 3600.0, 0.0,
-                nsteps, prm, lnk=lnk.astype(np.float32))
+                nsteps, prm, lnk=lnk.astype(np.float32), phys=phys)
     return p
 
 

@@ -6,8 +6,10 @@ set_amg right after it when precon_type = 1), set_grid, then the input and outpu
 `read_namelists` parses namelist text into {group: {name: value}}; `solver_params` turns
 the simulation, time and solution groups into the library's msg_params_t knobs the way
 the reference turns them into its own variables, and `grid_box` reads a grid file of type 7
-(corner and width per axis) into the box the library solves on.  Fields, boundary
-conditions and output settings are not read here.
+(corner and width per axis) into the box the library solves on.  `write_deck` writes a
+generated problem as a whole deck (msg123.main, grid, field, initial-head, region and
+time-series files) that the reference's own build reads, and `read_deck` reads such a deck
+back into a problem, fields, boundaries and all, scaled as the reference scales them.
 
 What follows the reference:
 * set_simulation (Read_input.f90:146-180): sim_type -1 steady, 0 long-term, 1 transient;
@@ -191,3 +193,308 @@ def grid_box(groups, grid_text):
     # glob_z(:,:,k) = zcorner + zwidth*(k-1), both products and the sum in real(SP)
     zs = [float(zc + zw * F32(k)) for k in range(nz + 1)]
     return nx, ny, nz, (abs(float(xw)), abs(float(yw)), abs(float(zw))), float(len_scale(max(abs(z) for z in zs)))
+
+
+# ---------------------------------------------------------------------------------------
+# Writing a deck: msg123.main and the files it names, for a generated problem
+# ---------------------------------------------------------------------------------------
+SNOVAL = -9999.0          # the reference's "no value" (Constval_module.f90:21,25)
+_SDATE = (2000, 1, 1, 0, 0, 0)
+
+
+def _fmt(v):
+    if isinstance(v, str):
+        return "'" + v.replace("'", "''") + "'"
+    if isinstance(v, bool):
+        return ".true." if v else ".false."
+    if isinstance(v, (list, tuple)):
+        return ", ".join(_fmt(x) for x in v)
+    if isinstance(v, (int, np.integer)):
+        return str(int(v))
+    return repr(float(v)).replace("e", "E")
+
+
+def namelist(name, **vals):
+    """One namelist group in the text form gfortran reads (&name, one name = value per line, /)."""
+    body = "".join(f"  {k} = {_fmt(v)}\n" for k, v in vals.items())
+    return f"&{name}\n{body}/\n"
+
+
+def _r4(path, arr):
+    np.asarray(arr, dtype="<f4").tofile(path)
+
+
+def write_deck(p, directory, end_time=None, sim_name="synthetic", outputs=("srat", "wtab", "mass"),
+               out_hours=1):
+    """Write msg123.main and the files it names into `directory` for a generated problem
+    (config.make_config), so that the reference's own build reads the same problem:
+
+    * set_simulation / set_calc_time (Read_input.f90:148-225): sim_type as in the problem,
+      time in seconds (calc_unit SEC); sim_type 1 runs from 2000-01-01 00:00:00 to the end
+      date end_time seconds later;
+    * set_calc_reg (:227-267): the whole grid (calc_type 0), or for a ponded top a 3D int32
+      region file (calc_type 6: -1 an inactive layer, 0 the sea layer, 1 the soil below --
+      the reference stops unless some cell is -1, Set_cell.f90:505-507);
+    * set_solution / set_amg (:337-395): steps in seconds, maxout_iter, maxinn_iter,
+      precon_type, criteria in metres (a relative criterion becomes criteria * max|h0|),
+      amg_nlevel, jac_omega, amg_theta;
+    * set_grid and a type-7 grid file (:397-583): corner and width per axis, z from the top
+      down (negative width);
+    * set_retn_parm (:618-663): compile files (inretn_type / inretn_path, inparm_type /
+      inparm_path, Open_file.f90:34-300) naming 3D float32 stream files (in_type 6) of
+      alpha, n, residual content, Ks x/y/z, Ss and saturated content, x fastest, top layer
+      first (Read_module.f90:459-485, flat_3d_3dr4);
+    * set_init (:665-713): the initial heads as a 3D float64 stream file (init_type 6);
+    * set_time_input: a time-series file (tinp_type / tinp_path / tinp_unit, :715-880)
+      with the rain as 2D float32 records in mm/h (rech_type 4, unit HOU: each record is its
+      float32 end time in hours followed by the field, Read_module.f90:skip_file), and the
+      sea head of a ponded top as a 3D float32 field, -9999 outside the sea layer (seal_type
+      6, no unit: constant);
+    * set_geog off, set_wtab 7, set_mass 7 (whole area), outputs every out_hours hours.
+
+    Refused (no counterpart in a deck): free drainage at the bottom and a fixed linear
+    tolerance.  Returns the list of files written."""
+    import os
+    ph = p.phys
+    if ph is None:
+        raise ValueError("the problem carries no unscaled inputs (phys)")
+    if p.free_drainage:
+        raise ValueError("free drainage at the bottom has no counterpart in a reference deck")
+    prm = p.params
+    if prm.get("lin_tol", 0.0) != 0.0:
+        raise ValueError("a fixed linear tolerance (lin_tol) has no counterpart in a reference deck")
+    os.makedirs(directory, exist_ok=True)
+    nx, ny, nz = p.nx, p.ny, p.nz
+    extra = 2 if p.sea_top else 0                   # inactive layer + sea layer above the soil
+    nzd = nz + extra
+    dx, dy, dz = ph["dx"], ph["dy"], ph["dz"]
+    z_grid = ph["z_top"] + extra * dz
+    if float(len_scale(z_grid)) != float(prm["len_scal"]):
+        raise ValueError("the deck's grid would change len_scal")
+    if extra and nx != ny:
+        # read_3d_calcreg places cell (i, j, k) at nx*ny*(k-1) + ny*(j-1) + i
+        # (Read_module.f90:1236), the grid index only when nx = ny
+        raise ValueError("a region file (ponded top) is read correctly by the reference only for nx = ny")
+    files = []
+    J = lambda name: os.path.join(directory, name)
+
+    def put(name, text):
+        with open(J(name), "w") as f:
+            f.write(text)
+        files.append(name)
+
+    def field3d(vals, fill):
+        full = np.empty(nx * ny * nzd, dtype=np.float64)
+        full[: extra * nx * ny] = fill
+        full[extra * nx * ny:] = vals
+        return full
+
+    # grid (type 7): header, then "corner width" for x, y (southward) and z (downward)
+    put("grid.txt", "corner width\n" + f"0.0 {dx!r}\n" + f"0.0 {dy!r}\n" + f"{z_grid!r} {-dz!r}\n")
+    # fields: the extra layers above the soil repeat the top soil layer's values
+    top = lambda a: np.tile(np.asarray(a)[: nx * ny], extra) if extra else np.zeros(0)
+    for key in ("alpha", "n", "resi", "ksx", "ksy", "ksz", "ss", "ths"):
+        a = np.asarray(ph[key], dtype=np.float32)
+        _r4(J(key + ".bin"), np.concatenate([top(a), a]))
+        files.append(key + ".bin")
+    put("retention.txt", namelist("inretn_type", vana_type=6, vann_type=6, resi_type=6)
+        + namelist("inretn_path", in_vapath="alpha.bin", in_vnpath="n.bin", in_repath="resi.bin"))
+    put("parameter.txt", namelist("inparm_type", pakx_type=6, paky_type=6, pakz_type=6, pass_type=6, pats_type=6)
+        + namelist("inparm_path", in_kxpath="ksx.bin", in_kypath="ksy.bin", in_kzpath="ksz.bin",
+                   in_sspath="ss.bin", in_tspath="ths.bin"))
+    field3d(np.asarray(ph["head0"], dtype=np.float64), SNOVAL).astype("<f8").tofile(J("init_head.bin"))
+    files.append("init_head.bin")
+    # calculation region
+    if extra:
+        reg = np.concatenate([np.full(nx * ny, -1, np.int32), np.zeros(nx * ny, np.int32),
+                              np.ones(nx * ny * nz, np.int32)])
+        reg.astype("<i4").tofile(J("region.bin"))
+        files.append("region.bin")
+        calc_reg = dict(calc_type=6, calcreg_neib=-1, calcreg_name="region.bin", inact_name="", clas_file="")
+    else:
+        calc_reg = dict(calc_type=0, calcreg_neib=-1, calcreg_name="", inact_name="", clas_file="")
+    # time series: rain (mm/h, records with their end time in hours) and the sea head
+    tt = dict(seal_type=-1, rech_type=-1, well_type=-1, weks_type=-1, weke_type=-1, rive_type=-1, lake_type=-1,
+              prec_type=-1, evap_type=-1)
+    tp = dict(seal_path="", rech_path="", well_path="", weks_path="", weke_path="", rive_path="", lake_path="",
+              prec_path="", evap_path="")
+    tu = dict(seal_unit="", rech_unit="", well_unit="", prec_unit="", evap_unit="")
+    if ph.get("rain_mm_h", 0.0) and ph.get("rain_hours", 0.0):
+        with open(J("rain.bin"), "wb") as f:
+            for t_end, v in ((ph["rain_hours"], ph["rain_mm_h"]), (1.0e30, 0.0)):
+                np.array([t_end], dtype="<f4").tofile(f)
+                np.full(nx * ny, v, dtype="<f4").tofile(f)
+        files.append("rain.bin")
+        tt["rech_type"], tp["rech_path"], tu["rech_unit"] = 4, "rain.bin", "HOU"
+    if extra:
+        sea = np.full(nx * ny * nzd, SNOVAL, dtype=np.float64)
+        sea[nx * ny: 2 * nx * ny] = ph["sea_head"]
+        _r4(J("sea_level.bin"), sea)
+        files.append("sea_level.bin")
+        tt["seal_type"], tp["seal_path"] = 6, "sea_level.bin"
+    put("timeseries.txt", namelist("tinp_type", **tt) + namelist("tinp_path", **tp) + namelist("tinp_unit", **tu))
+    # msg123.main
+    sim_type = int(prm.get("sim_type", 0))
+    if end_time is None:
+        end_time = prm["end_time"] if prm.get("end_time", 1.0e30) < 1.0e29 else p.nsteps * prm["max_step"]
+    if sim_type == 1:
+        end = datetime.datetime(*_SDATE) + datetime.timedelta(seconds=int(round(end_time)))
+        tm = dict(stime_type=0, sdate=list(_SDATE), edate=[end.year, end.month, end.day, end.hour, end.minute,
+                                                          end.second], end_time=0.0, calc_unit="SEC")
+    else:
+        tm = dict(stime_type=0, sdate=[0] * 6, edate=[0] * 6, end_time=float(end_time), calc_unit="SEC")
+    crit = float(prm["criteria"])
+    if prm.get("criteria_rel", 0):
+        crit = crit * float(np.max(np.abs(ph["head0"])))
+    sol = dict(init_step=float(prm["ini_step"]), incr_multi=float(prm["inc_fact"]), max_step=float(prm["max_step"]),
+               maxout_iter=int(prm["maxout_iter"]), criteria=crit, maxinn_iter=int(prm["maxinn_iter"]),
+               precon_type=int(prm["precon_type"]))
+    text = (namelist("set_simulation", sim_type=sim_type, sim_name=sim_name)
+            + namelist("set_calc_time", **tm)
+            + namelist("set_calc_reg", **calc_reg)
+            + namelist("set_solution", **sol))
+    if sol["precon_type"] == 1:
+        text += namelist("set_amg", amg_nlevel=int(prm["amg_nlevel"]), maxvcy_iter=1, max_sweep=int(prm["amg_sweeps"]),
+                         jac_omega=float(prm["jac_omega"]), amg_theta=float(prm["amg_theta"]))
+    text += (namelist("set_grid", gridx=nx, gridy=ny, gridz=nzd, grid_type=7, grid_file="grid.txt")
+             + namelist("set_retn_parm", retn_type=0, parm_type=0, retn_file="retention.txt",
+                        parm_file="parameter.txt")
+             + namelist("set_init", init_type=6, init_file="init_head.bin", init_dept=0.0, init_unit="")
+             + namelist("set_time_input", time_input_file="timeseries.txt")
+             + namelist("set_geog", geog_type=-1, geog_file="")
+             + namelist("set_wtab", wtab_type=7 if "wtab" in outputs else -1)
+             + namelist("set_mass", mass_type=7 if "mass" in outputs else -1, mass_file="")
+             + namelist("set_out_vari", out_list=",".join(outputs))
+             + namelist("set_out_unit", **{f"{v}_unit": "HOU" for v in _OUTV})
+             + namelist("set_out_time", **{f"{v}_time": int(out_hours) for v in _OUTV}))
+    put("msg123.main", text)
+    return files
+
+
+_OUTV = ("head", "rest", "srat", "wtab", "mass", "velc", "rivr", "lakr", "sufr", "dunr", "seal", "well", "rech")
+
+
+# ---------------------------------------------------------------------------------------
+# Reading a whole deck back into a problem
+# ---------------------------------------------------------------------------------------
+def _read_r4(path, n):
+    a = np.fromfile(path, dtype="<f4")
+    if a.size != n:
+        raise ValueError(f"{path}: {a.size} values, expected {n}")
+    return a
+
+
+def read_deck(directory):
+    """A problem (config.Problem, nondimensional like the generators) from a deck of the
+    kind write_deck produces: type-7 grid; whole-grid region, or an int32 region file of
+    layers (-1 inactive, 0 sea, 1 soil) with the sea layer directly above the soil; retention
+    and parameter compile files naming 3D float32 fields (in_type 6); initial heads as a 3D
+    float64 field (init_type 6); rain as 2D float32 records in mm/h with their end times
+    (rech_type 4) and a constant 3D float32 sea level (seal_type 6).  Scaling as the
+    reference applies it: alpha and Ss times len_scal, Ks times 1/len_scal in real(SP)
+    (Assign_calculation.f90:117,259-260); heads times 1/len_scal in real(DP)
+    (Assign_calculation.f90:471-473); sea heads real(SP) times 1/len_scal
+    (Assign_boundary.f90:155); elevations from the grid's real(SP) corner and width, then
+    times 1/len_scal in real(DP) (Read_input.f90:548-583, :1108-1110)."""
+    import os
+    from .config import Problem, default_params
+    J = lambda name: os.path.join(directory, name)
+    groups = read_namelists(open(J("msg123.main")).read())
+    prm = solver_params(groups)
+    g = groups["set_grid"]
+    nx, ny, nzd = int(g["gridx"]), int(g["gridy"]), int(g["gridz"])
+    if int(g.get("grid_type", -1)) != 7:
+        raise ValueError("only grid_type 7 (corner and width per axis) is read here")
+    lines = [l.split() for l in open(J(g["grid_file"])).read().splitlines() if l.strip()]
+    (xc, xw), (yc, yw), (zc, zw) = [(F32(float(a)), F32(float(b))) for a, b, *_ in lines[1:4]]
+    zs_m = np.array([zc + zw * F32(k) for k in range(nzd + 1)], dtype=F32)      # real(SP) node elevations
+    ls = len_scale(float(np.max(np.abs(zs_m.astype(np.float64)))))
+    lsi = F32(1.0) / ls
+    nxy = nx * ny
+    # region: whole grid, or layers of -1 (inactive), 0 (sea) and 1 (soil)
+    reg = groups["set_calc_reg"]
+    ct = int(reg.get("calc_type", -1))
+    if ct == 0:
+        flags = np.ones(nzd, np.int32)
+    elif ct == 6:
+        r = np.fromfile(J(reg["calcreg_name"]), dtype="<i4")
+        if r.size != nxy * nzd:
+            raise ValueError("region file size")
+        r = r.reshape(nzd, nxy)
+        if not all(np.all(r[k] == r[k, 0]) for k in range(nzd)):
+            raise ValueError("only layered regions are read here")
+        flags = r[:, 0]
+    else:
+        raise ValueError(f"calc_type {ct} is not read here")
+    soil = np.nonzero(flags > 0)[0]
+    k0, nz = int(soil[0]), len(soil)
+    if not np.array_equal(soil, np.arange(k0, k0 + nz)) or np.any(flags[k0 + nz:] != 1):
+        raise ValueError("the soil layers must be contiguous down to the bottom")
+    sea_top = int(k0 > 0 and flags[k0 - 1] == 0)
+    N = nxy * nz
+    sl = slice(k0 * nxy, (k0 + nz) * nxy)
+    # fields
+    rp = read_namelists(open(J(groups["set_retn_parm"]["retn_file"])).read())
+    pp = read_namelists(open(J(groups["set_retn_parm"]["parm_file"])).read())
+    for grp, keys in ((rp["inretn_type"], ("vana_type", "vann_type", "resi_type")),
+                      (pp["inparm_type"], ("pakx_type", "paky_type", "pakz_type", "pass_type", "pats_type"))):
+        if any(int(grp[k]) != 6 for k in keys):
+            raise ValueError("only 3D float32 fields (in_type 6) are read here")
+    path = lambda grp, k: J(grp[k])
+    f = {k: _read_r4(path(rp["inretn_path"], v), nxy * nzd)[sl]
+         for k, v in (("alpha", "in_vapath"), ("n", "in_vnpath"), ("resi", "in_repath"))}
+    f.update({k: _read_r4(path(pp["inparm_path"], v), nxy * nzd)[sl]
+              for k, v in (("ksx", "in_kxpath"), ("ksy", "in_kypath"), ("ksz", "in_kzpath"), ("ss", "in_sspath"),
+                           ("ths", "in_tspath"))})
+    ini = groups["set_init"]
+    if int(ini["init_type"]) != 6 or str(ini.get("init_unit", "")).strip():
+        raise ValueError("only an initial head file of in_type 6 without a time header is read here")
+    h_m = np.fromfile(J(ini["init_file"]), dtype="<f8")[sl]
+    # time series
+    ts = read_namelists(open(J(groups["set_time_input"]["time_input_file"])).read())
+    tt, tp, tu = ts["tinp_type"], ts["tinp_path"], ts.get("tinp_unit", {})
+    rain, rain_h = 0.0, 0.0
+    if int(tt.get("rech_type", -1)) > 0:
+        if int(tt["rech_type"]) != 4 or str(tu.get("rech_unit", "")).strip().upper() != "HOU":
+            raise ValueError("only rain as 2D float32 records with hourly end times is read here")
+        recs = np.fromfile(J(tp["rech_path"]), dtype="<f4").reshape(-1, nxy + 1)
+        if recs.shape[0] != 2 or np.any(recs[1, 1:] != 0) or np.any(recs[0, 1:] != recs[0, 1]):
+            raise ValueError("only a uniform rain followed by none is read here")
+        rain, rain_h = float(recs[0, 1]), float(recs[0, 0])
+    sea_head = None
+    if int(tt.get("seal_type", -1)) > 0:
+        if int(tt["seal_type"]) != 6 or not sea_top:
+            raise ValueError("only a constant 3D sea level over a sea layer is read here")
+        sv = _read_r4(J(tp["seal_path"]), nxy * nzd).reshape(nzd, nxy)[k0 - 1]
+        if np.any(sv != sv[0]):
+            raise ValueError("only a uniform sea level is read here")
+        sea_head = float(sv[0])
+    # geometry (uniform widths; elevations as the reference forms them)
+    z = zs_m.astype(np.float64) * float(lsi)
+    dxs = float(np.float64(F32(abs(xw))) * float(lsi))
+    dys = float(np.float64(F32(abs(yw))) * float(lsi))
+    top = np.repeat(z[k0:k0 + nz], nxy)
+    bot = np.repeat(z[k0 + 1:k0 + nz + 1], nxy)
+    hz = top - bot
+    dis = np.empty((6, N))
+    area = np.empty((6, N))
+    dis[0] = hz * 0.5; dis[5] = hz * 0.5
+    dis[1] = dys * 0.5; dis[4] = dys * 0.5
+    dis[2] = dxs * 0.5; dis[3] = dxs * 0.5
+    area[0] = dxs * dys; area[5] = dxs * dys
+    area[1] = dxs * hz; area[4] = dxs * hz
+    area[2] = dys * hz; area[3] = dys * hz
+    surf = top[:nxy].copy()
+    sc = lambda a, m: (np.asarray(a, F32) * (ls if m else lsi)).astype(F32)
+    rate = float(F32(rain * 1.0e-3 / 3600.0) * lsi)
+    prm = default_params(**dict(prm, len_scal=float(ls), criteria_rel=0, lin_tol=0.0))
+    sea = np.full(nxy, float(F32(sea_head) * lsi)) if sea_head is not None else np.zeros(nxy)
+    phys = dict(dx=float(abs(xw)), dy=float(abs(yw)), dz=float(abs(zw)), z_top=float(zs_m[k0]),
+                alpha=f["alpha"], n=f["n"], resi=f["resi"], ths=f["ths"], ss=f["ss"], ksx=f["ksx"], ksy=f["ksy"],
+                ksz=f["ksz"], head0=h_m, rain_mm_h=rain, rain_hours=rain_h, sea_head=sea_head)
+    return Problem("deck", nx, ny, nz, sea_top, 0, sc(f["alpha"], True), f["n"].astype(F32), f["resi"].astype(F32),
+                   f["ths"].astype(F32), sc(f["ss"], True), sc(f["ksx"], False), sc(f["ksy"], False),
+                   sc(f["ksz"], False), top, dxs * dys * hz, dis.reshape(-1).copy(), area.reshape(-1).copy(),
+                   np.full(nxy, dxs * dys), surf, surf.copy(), np.zeros(nxy), np.zeros(nxy), sea,
+                   h_m * float(lsi), rate * np.full(nxy, dxs * dys), rain_h * 3600.0 if rain_h else 1.0e30, 0.0,
+                   0, prm, phys=phys)
