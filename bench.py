@@ -138,7 +138,11 @@ def load_peaks(path=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks, power and clock-event reasons sampled every 200 ms during the timed region,
+    the fields nvidia-smi's clocks query reports, read through NVML in this process (a
+    thread of the sampler; no nvidia-smi process is started while the solver runs, so the
+    host side of the timed loop is not disturbed by process creation); nvidia-smi itself
+    when NVML cannot be loaded."""
 
     def __init__(self, index=0):
         self.index = index
@@ -146,7 +150,33 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml_sample(self, nv, h):
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        flag = lambda bit: "Active" if r & bit else "Not Active"
+        return [str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                str(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                "%.2f" % (nv.nvmlDeviceGetPowerUsage(h) / 1000.0),
+                flag(nv.nvmlClocksEventReasonHwSlowdown), flag(nv.nvmlClocksEventReasonHwThermalSlowdown),
+                flag(nv.nvmlClocksEventReasonSwThermalSlowdown), flag(nv.nvmlClocksEventReasonSwPowerCap)]
+
     def _run(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:
+            nv = None
+        if nv is not None:
+            try:
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(self._nvml_sample(nv, h))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.2)
+            finally:
+                nv.nvmlShutdown()
+            return
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -514,11 +544,12 @@ def main():
                        "msg_gpu_advance / msg_gpu_get_state (head_new, srat_new, surf_head), pinned host "
                        "buffers, host wall clock"}
         ge.close()
-        # ---- errors of the value path against plain FP64 on the same time steps ----------
+        # ---- errors of the value path against the converged FP64 answer -----------------
         # (the reference's method from the same state, each step forced to the value path's
-        # dt, so both solve the same discrete equations and differ by their arithmetic only)
+        # dt and solved to Newton criteria 1e-11 instead of 1e-8, so the difference is the
+        # value path's own error: its arithmetic and its stopping point)
         if not args.no_arms:
-            gf = GpuSolver(prob, **dict(ARMS[-1][1], sim_type=0, inc_fact=1.0))
+            gf = GpuSolver(prob, **dict(ARMS[-1][1], sim_type=0, inc_fact=1.0, criteria=1.0e-11, maxout_iter=60))
             gf.copy_state_from(gw)
             for dt in dts:
                 gf.set_state(delt=dt)
@@ -526,7 +557,8 @@ def main():
             head_d = gf.get_state(out={"head_new": np.zeros(prob.ncalc)})["head_new"]
             vol_d = water_volume(gf, head_d)
             inflow = inflow_volume(prob, t_start, t_end)
-            errors = {"against": "plain FP64 (reference method) on the value path's own time steps",
+            errors = {"against": "plain FP64 (reference method) solved to Newton criteria 1e-11 on the value "
+                                 "path's own time steps",
                       "steps": len(dts),
                       "head_rel": reduce(dist, float(np.max(np.abs(head_a - head_d)) / np.max(np.abs(head_d))), "max"),
                       "stored_water_rel_inflow": reduce(dist, abs(vol_a - vol_d) / inflow, "max"),

@@ -71,7 +71,7 @@ def test_config2_plain_prefix():
 
 def test_value_path_against_tight_fp64():
     """The benchmark's value path against the FP64 oracle solved to criteria 1e-11: heads
-    within 1e-8 after 8 and after 12 steps (measured 2.1e-9 and 2.3e-9); every step's
+    within 1e-8 after 8 and after 12 steps (measured 1.6e-9 and 2.8e-9); every step's
     volumes within 1e-10 of the step's inflow of the oracle's (measured <= 4e-12), and the
     GPU run's own mass balance closing to 1e-10 of the inflow (measured <= 4e-12)."""
     from msg123_b200.learned import Cnn
