@@ -20,7 +20,8 @@ time level (msg_gpu_copy_state) and covers the same window:
                  head), each with Newton/Krylov counts, rejections and simulated seconds.
                  The head and the stored water volume of the value path are compared with
                  the plain FP64 method run from the same state on the value path's own time
-                 steps (so both solve the same discrete equations).
+                 steps and solved to Newton criteria 1e-11 (the converged answer of the same
+                 discrete equations).  Every arm reports its device time per step by phase.
 * e2e          : the value path over the same K steps through the public C ABI with the
                  state in pinned host memory (set_state / advance / get_state each step,
                  copies inside the timed region, host wall clock).
@@ -290,8 +291,10 @@ def workload_config(args, prob):
             **({"overrides": dict(kv.split("=", 1) for kv in args.set)} if args.set else {})}
 
 
-def arm_stats(prob, st, ms, dist, fallbacks=None):
-    """Whole-job figures of one arm: value, counts per accepted step, simulated time."""
+def arm_stats(prob, st, ms, dist, fallbacks=None, timers=None):
+    """Whole-job figures of one arm: value, counts per accepted step, simulated time, and the
+    device time per accepted step of each phase the library times (assembly with the AMG
+    rebuilds, Krylov, AMG rebuilds alone, residual evaluations)."""
     acc = max(st["accepted"], 1)
     tmax = reduce(dist, ms, "max")
     out = {"value": reduce(dist, float(prob.ncalc * st["accepted"]), "sum") / (tmax * 1e-3),
@@ -301,6 +304,9 @@ def arm_stats(prob, st, ms, dist, fallbacks=None):
            "simulated_s_per_s": None}
     if fallbacks is not None:
         out["guess_fallbacks"], out["guess_rejected"] = fallbacks
+    if timers is not None:
+        out["phase_ms_per_step"] = {k[:-3]: round(timers[k] / acc, 3)
+                                    for k in ("assembly_ms", "krylov_ms", "amg_setup_ms", "residual_ms")}
     return out
 
 
@@ -356,9 +362,11 @@ class nvtx_range:
 
 def run_arm(g, steps):
     """Advance by `steps` accepted steps (or to the context's end time): (stats, device ms,
-    (learned guesses redone from the extrapolation, learned guesses not used))."""
+    (learned guesses redone from the extrapolation, learned guesses not used), the library's
+    per-phase device times)."""
     rc, st = g.advance(nsteps=steps)
-    return st, g.timers()["total_ms"], (g.guess_fallbacks(), g.guess_rejected())
+    tm = g.timers()
+    return st, tm["total_ms"], (g.guess_fallbacks(), g.guess_rejected()), tm
 
 
 def cpu_hw():
@@ -480,9 +488,9 @@ def main():
     barrier(dist)
     l0 = launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk, nvtx_range("value_window"):
-        st, ms, fb = run_arm(ga, K)
+        st, ms, fb, tm = run_arm(ga, K)
     launches = launch_count() - l0
-    value_arm = arm_stats(prob, st, ms, dist, fb)
+    value_arm = arm_stats(prob, st, ms, dist, fb, tm)
     value = value_arm["value"]
     tmax = value_arm["ms_per_step"] * max(st["accepted"], 1)
     t_end = st["current_t"]
@@ -507,8 +515,8 @@ def main():
         for name, kw in ARMS:
             barrier(dist)
             g = prep_arm(prob, kw, gw, cnn, end_time=t_end)
-            sta, msa, _ = run_arm(g, 4 * K)
-            arms[name] = arm_stats(prob, sta, msa, dist)
+            sta, msa, _, tma = run_arm(g, 4 * K)
+            arms[name] = arm_stats(prob, sta, msa, dist, timers=tma)
             g.close()
     for a in list(arms.values()) + [value_arm]:
         a["simulated_s_per_s"] = (a["simulated_s"] - t_start) / (a["ms_per_step"] * max(a["accepted"], 1) * 1e-3)

@@ -97,7 +97,7 @@ class _FakeSolver:
                        back_total=0, current_t=self.t, delt=600.0, status=0)
 
     def timers(self):
-        return {"total_ms": 10.0}
+        return {"assembly_ms": 3.0, "krylov_ms": 4.0, "amg_setup_ms": 1.0, "residual_ms": 2.0, "total_ms": 10.0}
 
     def kernel_time(self, which, reps=1):
         return {0: 0.01, 1: 0.02, 2: 0.03, 3: 0.05, 4: 1.0, 5: 0.2}[which]
