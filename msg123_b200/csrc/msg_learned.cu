@@ -458,6 +458,13 @@ static int cnn_forward_tc(Net &n, cudaStream_t s, const float **out, int withhol
 static double host_sumsq_diff(msg_ctx *c, const double *a, const double *b, int *rc) {
   const int B = kRedBlocks;
   k_sumsq_diff<<<B, 256, 0, c->stream>>>(c->N, a, b, c->part);
+  __atomic_fetch_add(&g_launches, 1LL, __ATOMIC_RELAXED);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("sumsq_diff launch: %s", cudaGetErrorString(e));
+    *rc = MSG_ERR_CUDA;
+    return 0.0;
+  }
   double t = 0.0;
   *rc = finish(c, B, 1, &t);
   return t;
