@@ -23,10 +23,10 @@ size_t conv_plan_plane(ConvPlan *plan);
 int conv_plan_load_compact(ConvPlan *plan, const __nv_bfloat16 *x, cudaStream_t s);
 
 // Four convolutions (GELU after the first three) from the plan's input buffer.
-// wpk: weights packed for the tensor cores, [layer][tap][k chunk][co][8 ci] bf16
-// (512 B per tap); bias: bias[l] points at 16 floats of layer l.  *out receives
-// the output channel in interior order (N floats, owned by the plan).
-// withhold >= 0 (tests only): the first layer never loads the box of that tile, so the
+// wpk: weights packed for the tensor cores by conv_pack_weights; bias: bias[l] points at
+// 16 floats of layer l.  *out receives the output channel in interior order (N floats,
+// owned by the plan).
+// withhold >= 0 (tests only): the first layer never loads the first box of that segment, so the
 // consumer's bounded wait runs out and the pass reports an error instead of hanging.
 int conv_forward_tc(ConvPlan *plan, const __nv_bfloat16 *wpk, const float *const bias[4], cudaStream_t s,
                     const float **out, int withhold = -1);
@@ -34,7 +34,9 @@ int conv_forward_tc(ConvPlan *plan, const __nv_bfloat16 *wpk, const float *const
 int conv_check(ConvPlan *plan, cudaStream_t s);
 
 // Pack W[tap][co][ci] (FP32 master weights, per-layer stride `layer_stride` floats) into
-// the tensor-core layout above.
+// the tensor-core layout of the z-march kernel: [layer][rotation][in-plane tap][k chunk]
+// [48 columns][8 ci] bf16, conv_packed_elems() elements.
+size_t conv_packed_elems();
 int conv_pack_weights(const float *w32, int layer_stride, __nv_bfloat16 *wpk, cudaStream_t s);
 
 }  // namespace msg

@@ -45,7 +45,7 @@ struct Net {
   float *w32 = nullptr;                // [kNParam] master weights
   __nv_bfloat16 *w16 = nullptr;        // [kLayers][kWl]  W[tap][co][ci]
   __nv_bfloat16 *wt16 = nullptr;       // [kLayers][kWl]  mirrored taps, transposed
-  __nv_bfloat16 *wtc = nullptr;        // [kLayers][kTaps][2][16][8] tensor-core operand layout
+  __nv_bfloat16 *wtc = nullptr;        // tensor-core operand layout (conv_pack_weights)
   ConvPlan *plan = nullptr;            // padded activations + TMA maps of the inference grid
   // One network may be attached to several contexts (e.g. ensemble members driven by
   // concurrent worker threads): the inference buffers are the network's, so each guess
@@ -548,7 +548,7 @@ MSG_API int msg_gpu_cnn_create(int32_t seed, msg_cnn_t **out) {
   MSG_CUDA(cudaMalloc(&n.grad, kNParam * 4));
   MSG_CUDA(cudaMalloc(&n.w16, kLayers * kWl * 2));
   MSG_CUDA(cudaMalloc(&n.wt16, kLayers * kWl * 2));
-  MSG_CUDA(cudaMalloc(&n.wtc, kLayers * kWl * 2));
+  MSG_CUDA(cudaMalloc(&n.wtc, conv_packed_elems() * 2));
   // every upload goes through the network's own (non-blocking) stream, so the kernels that
   // follow on that stream see it
   MSG_CUDA(cudaMemsetAsync(n.m, 0, kNParam * 4, n.stream));
