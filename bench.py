@@ -140,16 +140,33 @@ def load_peaks(path=None):
 
 class ClockSampler:
     """SM clocks, power and clock-event reasons sampled every 200 ms during the timed region,
-    the fields nvidia-smi's clocks query reports, read through NVML in this process (a
-    thread of the sampler; no nvidia-smi process is started while the solver runs, so the
-    host side of the timed loop is not disturbed by process creation); nvidia-smi itself
-    when NVML cannot be loaded."""
+    the fields nvidia-smi's clocks query reports, read through NVML in this process by a
+    thread of the sampler; nvidia-smi itself when NVML cannot be loaded.  NVML is
+    initialised when the sampler is made -- before the warm-up, not inside the timed region:
+    initialising it (as every nvidia-smi call does) can take the driver seconds on some
+    machines and held up the solver's own CUDA calls when it happened in the timed window."""
 
     def __init__(self, index=0):
         self.index = index
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self.nv = self.h = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.nv = nv
+        except Exception:
+            self.nv = None
+
+    def close(self):
+        if self.nv is not None:
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
+            self.nv = None
 
     def _nvml_sample(self, nv, h):
         r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
@@ -161,22 +178,14 @@ class ClockSampler:
                 flag(nv.nvmlClocksEventReasonSwThermalSlowdown), flag(nv.nvmlClocksEventReasonSwPowerCap)]
 
     def _run(self):
-        try:
-            import pynvml as nv
-            nv.nvmlInit()
-            h = nv.nvmlDeviceGetHandleByIndex(self.index)
-        except Exception:
-            nv = None
+        nv, h = self.nv, self.h
         if nv is not None:
-            try:
-                while not self._stop.is_set():
-                    try:
-                        self.samples.append(self._nvml_sample(nv, h))
-                    except Exception:
-                        pass
-                    self._stop.wait(0.2)
-            finally:
-                nv.nvmlShutdown()
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(self._nvml_sample(nv, h))
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
             return
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -475,6 +484,13 @@ def main():
     cnn = load(Cnn(seed=0))
     K = args.steps
 
+    # clock sampler (NVML) and torch (the NVTX range) set up before any timing
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    try:
+        import torch  # noqa: F401
+    except Exception:
+        pass
+
     # ---- warm-up on the value path; its time level is where every arm starts -----------
     gw = GpuSolver(prob, **FAST)
     cnn.attach(gw)
@@ -487,8 +503,9 @@ def main():
     ga = prep_arm(prob, FAST, gw, cnn)
     barrier(dist)
     l0 = launch_count()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk, nvtx_range("value_window"):
+    with clk, nvtx_range("value_window"):
         st, ms, fb, tm = run_arm(ga, K)
+    clk.close()
     launches = launch_count() - l0
     value_arm = arm_stats(prob, st, ms, dist, fb, tm)
     value = value_arm["value"]
