@@ -369,6 +369,27 @@ class nvtx_range:
             torch.cuda.nvtx.range_pop()
 
 
+def run_arm_steps(g, steps):
+    """run_arm one accepted step per call: the same work, timed per step (device time of
+    each step from the library's events; the sum is the arm's time), so that where a slow
+    window loses its time shows in the line."""
+    acc = {"accepted": 0, "rejected": 0, "newton_total": 0, "krylov_total": 0, "back_total": 0}
+    tm_sum = {"assembly_ms": 0.0, "krylov_ms": 0.0, "amg_setup_ms": 0.0, "residual_ms": 0.0, "total_ms": 0.0}
+    step_ms, st = [], None
+    while acc["accepted"] < steps:
+        rc, st = g.advance(nsteps=1)
+        tm = g.timers()
+        for k in acc:
+            acc[k] += st[k]
+        for k in tm_sum:
+            tm_sum[k] += tm[k]
+        step_ms.append(round(tm["total_ms"], 2))
+        if rc != 0 or st["accepted"] == 0:
+            break
+    out = dict(st, **acc)
+    return out, tm_sum["total_ms"], (g.guess_fallbacks(), g.guess_rejected()), tm_sum, step_ms
+
+
 def run_arm(g, steps):
     """Advance by `steps` accepted steps (or to the context's end time): (stats, device ms,
     (learned guesses redone from the extrapolation, learned guesses not used), the library's
@@ -504,10 +525,11 @@ def main():
     barrier(dist)
     l0 = launch_count()
     with clk, nvtx_range("value_window"):
-        st, ms, fb, tm = run_arm(ga, K)
+        st, ms, fb, tm, step_ms = run_arm_steps(ga, K)
     clk.close()
     launches = launch_count() - l0
     value_arm = arm_stats(prob, st, ms, dist, fb, tm)
+    value_arm["step_ms"] = step_ms
     value = value_arm["value"]
     tmax = value_arm["ms_per_step"] * max(st["accepted"], 1)
     t_end = st["current_t"]

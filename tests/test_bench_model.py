@@ -93,11 +93,15 @@ class _FakeSolver:
         while n < nsteps and self.t < self.params["end_time"]:
             self.t = min(self.t + 600.0, self.params["end_time"])
             n += 1
+        self.last_n = n
         return 0, dict(accepted=n, rejected=0, newton_total=5 * n, krylov_total=5 * n,
                        back_total=0, current_t=self.t, delt=600.0, status=0)
 
     def timers(self):
-        return {"assembly_ms": 3.0, "krylov_ms": 4.0, "amg_setup_ms": 1.0, "residual_ms": 2.0, "total_ms": 10.0}
+        """5 ms of device time per step of the last advance call."""
+        n = getattr(self, "last_n", 0)
+        return {"assembly_ms": 1.5 * n, "krylov_ms": 2.0 * n, "amg_setup_ms": 0.5 * n, "residual_ms": 1.0 * n,
+                "total_ms": 5.0 * n}
 
     def kernel_time(self, which, reps=1):
         return {0: 0.01, 1: 0.02, 2: 0.03, 3: 0.05, 4: 1.0, 5: 0.2}[which]
