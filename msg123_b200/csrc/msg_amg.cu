@@ -1211,7 +1211,29 @@ void amg_free(msg_ctx *c) {
   c->amg = nullptr;
 }
 
-int amg_setup(msg_ctx *c) {
+// Per-cell bytes of the arena reserved when a context is made: one hierarchy build of the
+// block workloads (levels, transfer operators, Galerkin temporaries) takes about 150 B per
+// fine cell; a build that outgrows the reservation spills to the pool and the arena is
+// enlarged at the next build, as before.
+constexpr size_t kArenaPerCell = 192;
+
+static int amg_state(msg_ctx *c);
+
+// Reserve the hierarchy's arena while the context is made, so that the first rebuilds of a
+// run allocate nothing: a multi-GB cudaMalloc inside a later rebuild took 50-150 ms more on
+// some machines than on others.
+int amg_reserve(msg_ctx *c) {
+  int rc;
+  if ((rc = amg_state(c))) return rc;
+  AmgState *A = S(c);
+  if (A->arena) return MSG_OK;
+  const size_t cap = (kArenaPerCell * (size_t)c->N + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
+  if (cudaMalloc((void **)&A->arena, cap) == cudaSuccess) A->arena_cap = cap;
+  else { A->arena = nullptr; A->arena_cap = 0; cudaGetLastError(); }   // the builds use the pool
+  return MSG_OK;
+}
+
+static int amg_state(msg_ctx *c) {
   int rc;
   AmgState *A = S(c);
   cudaStream_t s = c->stream;
@@ -1233,6 +1255,14 @@ int amg_setup(msg_ctx *c) {
     k_col0<<<nb(c->nnz), kThreads, 0, s>>>(c->nnz, c->offrow, A->col0);
     MSG_CHECK_LAUNCH();
   }
+  return MSG_OK;
+}
+
+int amg_setup(msg_ctx *c) {
+  int rc;
+  if ((rc = amg_state(c))) return rc;
+  AmgState *A = S(c);
+  cudaStream_t s = c->stream;
   for (size_t l = 1; l < A->lv.size(); ++l) free_level(A, A->lv[l], s);
   A->lv.clear();
   // reset the arena; enlarge it first when the previous build did not fit

@@ -618,6 +618,9 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
   if (p->precon_type == 0 || p->ref_quirks) {
     if ((rc = build_wavefront(c))) return rc;
   }
+  if (p->precon_type == 1 && !p->ref_quirks) {
+    if ((rc = amg_reserve(c))) return rc;
+  }
   MSG_CUDA(cudaStreamSynchronize(c->stream));
   return MSG_OK;
 }

@@ -132,6 +132,7 @@ int scale(msg_ctx *c, double *y, double a, int n);
 
 // ---- msg_amg.cu ---------------------------------------------------------------------------------
 int amg_setup(msg_ctx *c);
+int amg_reserve(msg_ctx *c);   // the hierarchy's device arena, reserved when the context is made
 int amg_apply(msg_ctx *c, const double *r, double *z);
 void amg_free(msg_ctx *c);
 

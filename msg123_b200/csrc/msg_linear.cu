@@ -261,17 +261,25 @@ __global__ void __launch_bounds__(256) k_abserrmax(int n, const double *xn, cons
   }
 }
 
-// lam_length of run_backtr (Nonlinear_solution.f90:503-512)
+// lam_length of run_backtr (Nonlinear_solution.f90:503-512): max(1, max_i |dh_i| / |h_i|) over
+// h_i != 0.  Rounding is monotone, so the largest rounded quotient is the rounding of the
+// largest exact one: each thread keeps the (numerator, denominator) pair of its largest
+// exact ratio, comparing a/b with c/d through a*d against c*b exactly (the rounded product
+// and its FMA error term), and divides once at the end -- the same value as dividing every
+// element, without an FP64 division per cell.
+__device__ __forceinline__ bool ratio_greater(double a, double b, double c, double d) {
+  const double p1 = a * d, p2 = c * b;
+  if (p1 != p2) return p1 > p2;
+  return fma(a, d, -p1) > fma(c, b, -p2);
+}
 __global__ void __launch_bounds__(256) k_lamlen(int n, const double *dh, const double *hn, double *part) {
   __shared__ double s[256];
-  double m = 1.0;
+  double num = 1.0, den = 1.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double h = hn[i];
-    if (h != 0.0) {
-      double t = __ddiv_rn(fabs(dh[i]), fabs(h));
-      if (t > m) m = t;
-    }
+    const double h = fabs(hn[i]), a = fabs(dh[i]);
+    if (h != 0.0 && ratio_greater(a, h, num, den)) { num = a; den = h; }
   }
+  const double m = __ddiv_rn(num, den);
   s[threadIdx.x] = m;
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
