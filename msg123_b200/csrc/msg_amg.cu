@@ -770,13 +770,33 @@ __global__ void k_jac_first_f(int n, const TB *b, const float *d, float w, float
 // First fine-level sweep from x = 0; also stores the FP32 rounding of the FP64 right-hand
 // side, which every later fine sweep of the cycle reads instead of rounding b again (the
 // same values, half the bytes).
-__global__ void k_jac_first_b(int n, const double *b, const float *d, float w, float *x, float *bf) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float bi = (float)b[i];
-    bf[i] = bi;
-    x[i] = (w * bi) / d[i];
+// Four elements per thread, all loads issued before the stores: 48 B in flight per thread
+// instead of 12, which the one-element form lacked to cover the HBM latency (138 us at
+// 25.2M cells, 3.6 TB/s).  Launch with grid4(n, block).
+__global__ void k_jac_first_b(int n, const double *__restrict__ b, const float *__restrict__ d, float w,
+                              float *__restrict__ x, float *__restrict__ bf) {
+  const int st = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * st) {
+    double bv[4];
+    float dv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * st;
+      bv[u] = i < n ? b[i] : 0.0;
+      dv[u] = i < n ? d[i] : 1.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * st;
+      if (i < n) {
+        const float bi = (float)bv[u];
+        bf[i] = bi;
+        x[i] = (w * bi) / dv[u];
+      }
+    }
   }
 }
+static int grid4(long long n, int block) { return (int)std::max(1LL, (n + 4LL * block - 1) / (4LL * block)); }
 __global__ void k_b2f(int n, const double *b, float *bf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) bf[i] = (float)b[i];
 }
@@ -787,27 +807,6 @@ __global__ void k_b2f(int n, const double *b, float *bf) {
 // products of a lane are added in entry order.  Every lane reaches the shuffles.
 __device__ __forceinline__ float ldf(const float *p) { return *p; }
 __device__ __forceinline__ float ldf(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
-// Sequential sum of one CSR row of float weights against a gathered vector, loads issued
-// four entries at a time (same order of additions as the plain loop).
-__device__ __forceinline__ float csr_row_f4(int beg, int end, const int *cl, const float *val, const float *x) {
-  float s = 0.f;
-  for (int k = beg; k < end; k += 4) {
-    int c[4];
-    float a[4], xv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int kk = k + u;
-      c[u] = kk < end ? cl[kk] : -1;
-      a[u] = kk < end ? val[kk] : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (c[u] >= 0) s += a[u] * xv[u];
-  }
-  return s;
-}
 // Two rows per quad: the quad walks rows 2Q and 2Q+1 together (column and value loads of
 // both rows, then the gathers of both), so a warp keeps sixteen rows' loads in flight
 // (4% off the mixed V-cycle at 25.2M cells against one row per quad).  Launch with
@@ -884,6 +883,69 @@ __global__ void k_res_csr_h(int n, const int *rp, const int *cl, const __nv_bflo
 }
 // 4 threads per two rows
 static int grid2r(int n) { return (int)((((long long)n + 1) / 2 * 4 + kThreads - 1) / kThreads); }
+
+// Block-streamed CSR passes of the mixed V-cycle's coarse levels and transfers (the
+// CSR-stream scheme of Greathouse and Daga, "Efficient sparse matrix-vector multiplication
+// on GPUs using the CSR storage format", SC 2014).  A block owns kSR consecutive rows,
+// whose entries are one contiguous range of the CSR arrays: the block walks that range in
+// chunks of kSC entries with consecutive threads on consecutive entries (column and value
+// loads coalesced, four entries per thread issued before their gathers), parks the
+// products in shared memory, and each thread then adds its own row's products in entry
+// order.  Rows of any length are handled by the chunk loop.
+constexpr int kSR = 128, kSC = 2048, kSU = 4;
+enum { kCsrJacobi = 0, kCsrResidual = 1, kCsrRowSum = 2, kCsrAddTo = 3 };
+// OP kCsrJacobi: y_i = x_i + w (b_i - d_i x_i - sum_k v_k x_{c_k}) / d_i
+// OP kCsrResidual: y_i = b_i - d_i x_i - sum_k v_k x_{c_k}
+// OP kCsrRowSum: y_i = sum_k v_k x_{c_k}               (restriction, R = P^T)
+// OP kCsrAddTo: y_i = y_i + sum_k v_k x_{c_k}          (prolongation, x += P x_c)
+template <int OP, typename TV>
+__global__ void __launch_bounds__(kSR) k_csr_stream(int n, const int *__restrict__ rp, const int *__restrict__ cl,
+                                                    const TV *__restrict__ v, const float *__restrict__ d,
+                                                    const float *__restrict__ b, float w, const float *__restrict__ x,
+                                                    float *y) {
+  __shared__ float prod[kSC];
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * kSR, i = i0 + t;
+  const bool own = i < n;
+  const int beg = rp[i0], end = rp[min(i0 + kSR, n)];
+  int rb = 0, re = 0;
+  float bi = 0.f, di = 1.f, xi = 0.f;
+  if (own) {
+    rb = rp[i];
+    re = rp[i + 1];
+    if (OP == kCsrJacobi || OP == kCsrResidual) { bi = b[i]; di = d[i]; xi = x[i]; }
+    if (OP == kCsrAddTo) xi = y[i];
+  }
+  float s = 0.f;
+  for (int c0 = beg; c0 < end; c0 += kSC) {
+    const int c1 = min(c0 + kSC, end);
+    for (int k = c0 + t; k < c1; k += kSR * kSU) {
+      int cc[kSU];
+      float a[kSU], xv[kSU];
+#pragma unroll
+      for (int u = 0; u < kSU; ++u) {
+        const int kk = k + u * kSR;
+        cc[u] = kk < c1 ? cl[kk] : -1;
+        a[u] = kk < c1 ? ldf(v + kk) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < kSU; ++u) xv[u] = cc[u] >= 0 ? x[cc[u]] : 0.f;
+#pragma unroll
+      for (int u = 0; u < kSU; ++u)
+        if (cc[u] >= 0) prod[k + u * kSR - c0] = a[u] * xv[u];
+    }
+    __syncthreads();
+    const int lo = max(rb, c0), hi = min(re, c1);
+    for (int k = lo; k < hi; ++k) s += prod[k - c0];
+    __syncthreads();
+  }
+  if (!own) return;
+  if (OP == kCsrJacobi) y[i] = xi + (w * (bi - (di * xi + s))) / di;
+  else if (OP == kCsrResidual) y[i] = bi - (di * xi + s);
+  else if (OP == kCsrRowSum) y[i] = s;
+  else y[i] = xi + s;
+}
+static int gridS(int n) { return (n + kSR - 1) / kSR; }
 // Restriction b_c = R r: a coarse row gathers from every fine row its aggregate's
 // smoothed prolongation reaches (tens of entries), so it is split over four lanes like the
 // coarse-level smoother.  Launch with grid2r(nc).
@@ -895,10 +957,84 @@ __global__ void k_restrict_f(int nc, const int *rp, const int *rc, const float *
   const int I = I0 + (q & 1);
   if (q < 2 && I < nc) bc[I] = q ? t1 : t0;
 }
-__global__ void k_prolong_f(int nf, const int *pp, const int *pc, const float *pv, const float *xc, float *x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
-    const float xi = x[i];
-    x[i] = xi + csr_row_f4(pp[i], pp[i + 1], pc, pv, xc);
+// Prolongation x += P x_c, a thread per fine row, four rows per thread (rows i0 + u*stride):
+// the row bounds, the own values, the first entry of each row and its gather are issued for
+// all four rows before any sum (prolongation rows hold 0 to 3 entries, most one or none);
+// the rest of a row continues the same in-order sum.  Launch with grid4(nf, block).
+__device__ __forceinline__ float csr_row_from(float s, int beg, int end, const int *cl, const float *val,
+                                              const float *x) {
+  for (int k = beg; k < end; k += 4) {
+    int c[4];
+    float a[4], xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int kk = k + u;
+      c[u] = kk < end ? cl[kk] : -1;
+      a[u] = kk < end ? val[kk] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (c[u] >= 0) s += a[u] * xv[u];
+  }
+  return s;
+}
+__global__ void k_prolong_f(int nf, const int *__restrict__ pp, const int *__restrict__ pc,
+                            const float *__restrict__ pv, const float *__restrict__ xc, float *x) {
+  const int st = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < nf; i0 += 4 * st) {
+    int beg[4], end[4], c[4];
+    float a[4], g[4], xi[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * st;
+      const bool live = i < nf;
+      beg[u] = live ? pp[i] : 0;
+      end[u] = live ? pp[i + 1] : 0;
+      xi[u] = live ? x[i] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      c[u] = beg[u] < end[u] ? pc[beg[u]] : -1;
+      a[u] = beg[u] < end[u] ? pv[beg[u]] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) g[u] = c[u] >= 0 ? xc[c[u]] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * st;
+      if (i < nf) {
+        float s = 0.f;
+        if (c[u] >= 0) s += a[u] * g[u];
+        if (beg[u] + 1 < end[u]) s = csr_row_from(s, beg[u] + 1, end[u], pc, pv, xc);
+        x[i] = xi[u] + s;
+      }
+    }
+  }
+}
+// One coarse-level CSR pass.  Measured per pass at 25.2M cells (levels of 2.78M rows x 14
+// entries, 204k x 44, 22k x 48, ...): the block-streamed kernel takes 94.6 us per Jacobi
+// sweep of the 2.78M-row level against 107.4 for four lanes per row, and 49.6 against 59.4
+// for the restriction onto it (5.7 entries per row), but is slower on the short, dense
+// levels (28.1 against 24.4 us at 204k rows, 16.1 against 7.8 at 22k) and for the
+// prolongation rows (0.6 to 3 entries; 148 against 125 us on the fine grid).  So: long
+// levels of short rows stream, the rest runs four lanes per row, prolongation a thread
+// per row.
+template <int OP, typename TV>
+static void csr_pass(int n, int nnz, const int *rp, const int *cl, const TV *v, const float *d, const float *b,
+                     float w, const float *x, float *y, cudaStream_t s) {
+  const bool stream = OP != kCsrAddTo && n >= (1 << 19) && (long long)nnz <= 24LL * n;
+  if (stream) {
+    k_csr_stream<OP, TV><<<gridS(n), kSR, 0, s>>>(n, rp, cl, v, d, b, w, x, y);
+  } else if constexpr (OP == kCsrJacobi) {
+    k_jac_csr_h<<<grid2r(n), kThreads, 0, s>>>(n, rp, cl, v, d, b, w, x, y);
+  } else if constexpr (OP == kCsrResidual) {
+    k_res_csr_h<<<grid2r(n), kThreads, 0, s>>>(n, rp, cl, v, d, b, x, y);
+  } else if constexpr (OP == kCsrRowSum) {
+    k_restrict_f<<<grid2r(n), kThreads, 0, s>>>(n, rp, cl, v, x, y);
+  } else {
+    k_prolong_f<<<grid4(n, kThreads), kThreads, 0, s>>>(n, rp, cl, v, x, y);
   }
 }
 // coarsest level: FP64 dense inverse applied to a float right-hand side, one warp per
@@ -1402,24 +1538,24 @@ static int vcycle_f(msg_ctx *c, int l, const float *b, float *x) {
     k_jac_first_f<float><<<g, kThreads, 0, s>>>(n, b, L.diag_f, w, cur);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
-      k_jac_csr_h<<<grid2r(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+      csr_pass<kCsrJacobi>(n, L.nnz, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth, s);
       MSG_CHECK_LAUNCH();
       std::swap(cur, oth);
     }
   }
   if (!last) {
     AmgLevel &C = A->lv[l + 1];
-    k_res_csr_h<<<grid2r(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, cur, L.rf);
+    csr_pass<kCsrResidual>(n, L.nnz, L.rowptr, L.col, L.val_h, L.diag_f, b, 0.f, cur, L.rf, s);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<grid2r(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, L.rf, C.bf);
+    csr_pass<kCsrRowSum>(C.n, C.pnnz, C.rptr, C.rcol, C.rval_f, nullptr, nullptr, 0.f, L.rf, C.bf, s);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, l + 1, C.bf, C.xf);
     if (rc) return rc;
-    k_prolong_f<<<g, kThreads, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
+    csr_pass<kCsrAddTo>(n, C.pnnz, C.pptr, C.pcol, C.pval_f, nullptr, nullptr, 0.f, C.xf, cur, s);
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {
-    k_jac_csr_h<<<grid2r(n), kThreads, 0, s>>>(n, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth);
+    csr_pass<kCsrJacobi>(n, L.nnz, L.rowptr, L.col, L.val_h, L.diag_f, b, w, cur, oth, s);
     MSG_CHECK_LAUNCH();
     std::swap(cur, oth);
   }
@@ -1446,7 +1582,7 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
     k_b2f<<<gs, bs, 0, s>>>(n, b, bf);
     MSG_CHECK_LAUNCH();
   } else {
-    k_jac_first_b<<<gs, bs, 0, s>>>(n, b, c->dmat_f, w, cur, bf);
+    k_jac_first_b<<<grid4(n, bs), bs, 0, s>>>(n, b, c->dmat_f, w, cur, bf);
     MSG_CHECK_LAUNCH();
     for (int k = 1; k < sw; ++k) {
       k_jac_dia3<float><<<g3, b3, 0, s>>>(D, bf, w, cur, oth);
@@ -1458,11 +1594,11 @@ static int vcycle_mixed(msg_ctx *c, const double *b, double *z) {
     AmgLevel &C = A->lv[1];
     k_res_dia3<<<g3, b3, 0, s>>>(D, bf, cur, A->r0f);
     MSG_CHECK_LAUNCH();
-    k_restrict_f<<<grid2r(C.n), kThreads, 0, s>>>(C.n, C.rptr, C.rcol, C.rval_f, A->r0f, C.bf);
+    csr_pass<kCsrRowSum>(C.n, C.pnnz, C.rptr, C.rcol, C.rval_f, nullptr, nullptr, 0.f, A->r0f, C.bf, s);
     MSG_CHECK_LAUNCH();
     int rc = vcycle_f(c, 1, C.bf, C.xf);
     if (rc) return rc;
-    k_prolong_f<<<gs, bs, 0, s>>>(n, C.pptr, C.pcol, C.pval_f, C.xf, cur);
+    csr_pass<kCsrAddTo>(n, C.pnnz, C.pptr, C.pcol, C.pval_f, nullptr, nullptr, 0.f, C.xf, cur, s);
     MSG_CHECK_LAUNCH();
   }
   for (int k = 0; k < sw; ++k) {

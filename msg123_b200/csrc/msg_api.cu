@@ -176,6 +176,11 @@ static int calc_funcl2norm(msg_ctx *c, double in_lam) {
 }
 
 // run_backtr (Nonlinear_solution.f90:441-631)
+// The line-search slope reads the right-hand side assembled for this Newton iteration,
+// which nothing changes before the slope is taken -- except with the reference's AMG
+// quirks, where the preconditioner leaves its input there (Q2) and slope_rhs holds it.
+static bool slope_from_rhs(const msg_ctx *c) { return !(c->prm.precon_type == 1 && c->prm.ref_quirks); }
+
 static int run_backtr(msg_ctx *c) {
   const int n = c->N;
   const double back_alpha = 1.0e-4, back_beta = 0.9;
@@ -187,28 +192,34 @@ static int run_backtr(msg_ctx *c) {
   // taken before F(head_new) so that the last residual evaluation of the line search is
   // always the one at the accepted head_new (its S and kr stay current; calc_numsol reuses it)
   double *jacvec = c->tmpv;
-  if (c->prm.jv_mode == 1 && !c->prm.ref_quirks) {
-    // J.dh of the assembled Jacobian: BiCGStab started from dh = 0 and keeps r = rhs - J dh
-    if ((rc = axpby(c, jacvec, c->rhs, -1.0, c->r, n))) return rc;
-  } else if ((rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) {
-    return rc;
-  }
+  // J.dh of the assembled Jacobian (jv_mode 1): BiCGStab started from dh = 0 and keeps
+  // r = rhs - J dh, so the slope below is (rhs, rhs - r), formed in one pass
+  const bool jv_resid = c->prm.jv_mode == 1 && !c->prm.ref_quirks;
+  if (!jv_resid && (rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) return rc;
   double dummy;
   if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
-  double l2_pnorm;
-  if ((rc = dot(c, c->head_change, c->head_change, n, &l2_pnorm))) return rc;
+  // ||dh||^2, ||F(head_new)||^2, the slope and lam_length in one pass; lam_length is taken
+  // again if dh is shortened (the slope, from J dh of the unshortened step, is scaled below)
+  const double *srhs = slope_from_rhs(c) ? c->rhs : c->slope_rhs;   // or (Q2) the last preconditioner input
+  double stats[4];
+  if ((rc = backtr_stats(c, c->head_change, c->head_new, c->new_f, srhs, jv_resid ? nullptr : jacvec, c->rhs, c->r,
+                         stats)))
+    return rc;
+  const double l2_pnorm = stats[0];
+  c->l2_new = stats[1];
+  double slope = stats[2];
+  lam_len = stats[3];
   double sql2_pnorm = std::sqrt(l2_pnorm);
+  bool scaled = false;
   if (sql2_pnorm > c->maxstep) {
     maxpnorm = c->maxstep / sql2_pnorm;
     if ((rc = scale(c, c->head_change, maxpnorm, n))) return rc;
     sql2_pnorm = c->maxstep;
+    scaled = true;
   }
   double step_len = sql2_pnorm;
-  if ((rc = dot(c, c->new_f, c->new_f, n, &c->l2_new))) return rc;
-  double slope;
-  if ((rc = dot(c, c->slope_rhs, jacvec, n, &slope))) return rc;
   slope = slope * maxpnorm;
-  if ((rc = lam_length(c, c->head_change, c->head_new, &lam_len))) return rc;
+  if (scaled && (rc = lam_length(c, c->head_change, c->head_new, &lam_len))) return rc;
   c->l2_jnorm = c->l2_jnorm * maxpnorm * maxpnorm;
   double step_tol = std::pow(MACHI_EPS, 2.0 / 3.0);
   double lam_min = step_tol / lam_len;
@@ -356,16 +367,19 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     // them at head_new (the chosen guess was the last one evaluated)
     if ((rc = make_matvec(c, &l2r, c->out_iter > 1 || c->vg_at_head))) return rc;
     c->vg_at_head = 0;
-    if ((rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
+    if (!slope_from_rhs(c) && (rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
     if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }
-    if ((rc = copy_d2d(c, c->head_pre, c->head_new, n))) return rc;
-    MSG_CUDA(cudaMemsetAsync(c->head_change, 0, (size_t)n * 8, c->stream));
+    // head_pre takes the iterate by a buffer swap: nothing reads head_new again before
+    // head_new = head_pre + dh overwrites all of it (in check_abserrmax's pass)
+    std::swap(c->head_pre, c->head_new);
+    // dh starts at zero; BiCGStab's first update writes it without reading it
+    if (c->prm.maxinn_iter < 1) MSG_CUDA(cudaMemsetAsync(c->head_change, 0, (size_t)n * 8, c->stream));
     c->conv_flag = 0;
     c->errtol = c->prm.lin_tol > 0 ? c->prm.lin_tol : c->eta;
     if ((rc = solve_linalg(c, c->l2_pre, c->head_change, &c->l2_jnorm, true))) return rc;   // from dh = 0
     st.inner_total += c->in_iter; st.in_iter_last = c->in_iter;
-    if ((rc = axpby(c, c->head_new, c->head_pre, 1.0, c->head_change, n))) return rc;
-    if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
+    // head_new = head_pre + dh, formed inside check_abserrmax's pass
+    if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan, c->head_change))) return rc;
     check_val = std::fabs(c->maxvar) * c->len_scal;
     maxunk = std::fabs(maxunk) * c->len_scal;
     double crit = c->prm.criteria_rel ? c->prm.criteria * maxunk : c->prm.criteria;
@@ -606,11 +620,13 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
     ALLOC(c->dmat_f, N * 4);
     ALLOC(c->lu_f, 6 * N * 4);
   }
-  size_t npart = std::max((size_t)kRedBlocks * 8, 2 * (size_t)nblk((int)N) + 64);
+  // up to four arrays of one partial per block of 256 cells (the line search's k_backtr_stats)
+  size_t npart = std::max((size_t)kRedBlocks * 8, 4 * (size_t)nblk((int)N) + 64);
   // the flux passes' 3D grid can have more blocks than nblk(N) when nx or ny is not a
   // multiple of the tile (32 x 8)
   npart = std::max(npart, (size_t)((g->nx + 31) / 32) * ((g->ny + 7) / 8) * g->nz + 64);
   ALLOC(c->part, npart * 8);
+  c->npart = npart;
   ALLOC(c->dres, 16 * 8);
   MSG_CUDA(cudaMallocHost((void **)&c->hpin, (size_t)kRedBlocks * 8 * 8));
   int rc = build_connectivity(c, g);

@@ -59,7 +59,8 @@ struct msg_ctx {
   double *dilu_d, *r, *rs, *p, *v, *t, *z;
   msg::DevScalars *sc;                           // device scalars
   msg::DevScalars *sc_host;                      // pinned mirror
-  double *part;                                  // reduction partials [kRedBlocks * 8]
+  double *part;                                  // reduction partials [npart]
+  size_t npart;
   double *hpin;                                  // pinned host scalars
   double *dres;                                  // device reduction results [16]
   // ---- wavefront ordering for DILU --------------------------------------------------------
@@ -125,8 +126,12 @@ int dot(msg_ctx *c, const double *a, const double *b, int n, double *out);   // 
 // sum narr partial arrays (nparts each, consecutive in c->part) on the device; sync; host values
 int finish(msg_ctx *c, int nparts, int narr, double *out);
 int norm1(msg_ctx *c, const double *a, int n, double *out);
-int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan);
+int abserrmax(msg_ctx *c, double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan,
+              const double *dh = nullptr);   // dh: form xn = xp + dh first
 int lam_length(msg_ctx *c, const double *dh, const double *hn, double *out);
+// ||dh||^2, ||f||^2, (s, jv) (jv null: (s, b - r)) and lam_length(dh, hn) in one pass
+int backtr_stats(msg_ctx *c, const double *dh, const double *hn, const double *f, const double *s, const double *jv,
+                 const double *b, const double *r, double out[4]);
 int axpby(msg_ctx *c, double *y, const double *x, double a, const double *w, int n);   // y = x + a*w
 int scale(msg_ctx *c, double *y, double a, int n);
 

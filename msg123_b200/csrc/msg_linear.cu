@@ -147,20 +147,24 @@ int launch_spmv(msg_ctx *c, const double *x, double *y) {
 // ---------------------------------------------------------------------------------
 // Vector kernels with fused reductions (fixed grid -> deterministic partials).
 // ---------------------------------------------------------------------------------
-// p = r + beta*(p - omega*v)
-__global__ void k_bicg_p(int n, double *p, const double *r, const double *v, double beta, double omega) {
+// p = r + beta*(pin - omega*v)  (pin: the previous direction, p itself after the first update)
+__global__ void k_bicg_p(int n, const double *pin, double *p, const double *r, const double *v, double beta,
+                         double omega) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = __dadd_rn(r[i], __dmul_rn(beta, __dsub_rn(p[i], __dmul_rn(omega, v[i]))));
+    p[i] = __dadd_rn(r[i], __dmul_rn(beta, __dsub_rn(pin[i], __dmul_rn(omega, v[i]))));
 }
 
-// x += a*z; r -= a*w; partials ||r||^2 and (r, rs)
-__global__ void __launch_bounds__(256) k_bicg_xr(int n, double *x, double *r, const double *z, const double *w,
-                                                 const double *rs, double a, double *part) {
+// x = xin + a*z; r = rin - a*w; partials ||r||^2 and (r, rs).  xin null: x starts at zero
+// (0 + a*z, the value the zeroed x gave, without reading it); rin: the residual before the
+// update (the right-hand side itself on the first update from x = 0).
+__global__ void __launch_bounds__(256) k_bicg_xr(int n, const double *xin, double *x, const double *rin, double *r,
+                                                 const double *z, const double *w, const double *rs, double a,
+                                                 double *part) {
   __shared__ double sh[8];
   double s0 = 0.0, s1 = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] = __dadd_rn(x[i], __dmul_rn(a, z[i]));
-    double ri = __dsub_rn(r[i], __dmul_rn(a, w[i]));
+    x[i] = __dadd_rn(xin ? xin[i] : 0.0, __dmul_rn(a, z[i]));
+    double ri = __dsub_rn(rin[i], __dmul_rn(a, w[i]));
     r[i] = ri;
     s0 = __dadd_rn(s0, __dmul_rn(ri, ri));
     s1 = __dadd_rn(s1, __dmul_rn(ri, rs[i]));
@@ -184,24 +188,6 @@ __global__ void __launch_bounds__(256) k_dot2(int n, const double *a, const doub
     t = block_sum<256>(s1, sh);
     if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = t;
   }
-}
-
-// Start of BiCGStab from x = 0: r = r* = p = b and the partials of <r, r*> -- the same
-// values (b - A.0 = b) and the same per-block partials as the residual SpMV, two copies
-// and k_dot2 it replaces.
-__global__ void __launch_bounds__(256) k_bicg_start0(int n, const double *b, double *r, double *rs, double *p,
-                                                     double *part) {
-  __shared__ double sh[8];
-  double s0 = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double v = b[i];
-    r[i] = v;
-    rs[i] = v;
-    p[i] = v;
-    s0 = __dadd_rn(s0, __dmul_rn(v, v));
-  }
-  double t = block_sum<256>(s0, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 __global__ void __launch_bounds__(256) k_norm1(int n, const double *a, double *part) {
@@ -231,13 +217,22 @@ __device__ __forceinline__ ArgMax amax(ArgMax p, ArgMax q) {
   return p;
 }
 
-__global__ void __launch_bounds__(256) k_abserrmax(int n, const double *xn, const double *xp, double *part) {
+// dh non-null: first forms xn = xp + 1*dh (the Newton update, the axpby it replaces, same
+// rounding) and writes it, so xn is not read back.
+__global__ void __launch_bounds__(256) k_abserrmax(int n, double *xn, const double *xp, const double *dh,
+                                                   double *part) {
   __shared__ ArgMax s1[256], s2[256];
   __shared__ int snan[256];
   ArgMax c = {0.0, 0.0, -1}, x = {0.0, 0.0, -1};
   int nan = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double v = xn[i];
+    double v;
+    if (dh) {
+      v = __dadd_rn(xp[i], __dmul_rn(1.0, dh[i]));
+      xn[i] = v;
+    } else {
+      v = xn[i];
+    }
     if (v != v) nan = 1;
     double dv = __dsub_rn(v, xp[i]);
     c = amax(c, ArgMax{fabs(dv), dv, i});
@@ -299,9 +294,12 @@ static int fetch_partials(msg_ctx *c, int count) {
 // order, so every result repeats bit for bit: each thread keeps eight running sums over
 // the strided elements (eight loads in flight instead of one dependent chain), combines
 // them in a fixed tree, then the block reduces in a fixed tree.
+// MAXB: bit a set -> block a takes the maximum of its array instead of the sum.
+template <int MAXB = 0>
 __global__ void __launch_bounds__(1024) k_finish(const double *part, int nparts, double *out) {
   __shared__ double sh[1024];
   const double *p = part + (size_t)blockIdx.x * nparts;
+  const bool mx = (MAXB >> blockIdx.x) & 1;
   constexpr int U = 8;
   double a[U];
 #pragma unroll
@@ -310,15 +308,18 @@ __global__ void __launch_bounds__(1024) k_finish(const double *part, int nparts,
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = base + u * blockDim.x;
-      if (i < nparts) a[u] = __dadd_rn(a[u], p[i]);
+      if (i < nparts) a[u] = mx ? fmax(a[u], p[i]) : __dadd_rn(a[u], p[i]);
     }
   }
-  const double s = __dadd_rn(__dadd_rn(__dadd_rn(a[0], a[1]), __dadd_rn(a[2], a[3])),
-                             __dadd_rn(__dadd_rn(a[4], a[5]), __dadd_rn(a[6], a[7])));
+  double s;
+  if (mx) s = fmax(fmax(fmax(a[0], a[1]), fmax(a[2], a[3])), fmax(fmax(a[4], a[5]), fmax(a[6], a[7])));
+  else s = __dadd_rn(__dadd_rn(__dadd_rn(a[0], a[1]), __dadd_rn(a[2], a[3])),
+                     __dadd_rn(__dadd_rn(a[4], a[5]), __dadd_rn(a[6], a[7])));
   sh[threadIdx.x] = s;
   __syncthreads();
   for (int o = 512; o > 0; o >>= 1) {
-    if ((int)threadIdx.x < o) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + o]);
+    if ((int)threadIdx.x < o)
+      sh[threadIdx.x] = mx ? fmax(sh[threadIdx.x], sh[threadIdx.x + o]) : __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + o]);
     __syncthreads();
   }
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
@@ -345,8 +346,9 @@ int norm1(msg_ctx *c, const double *a, int n, double *out) {
   return finish(c, nblk(n), 1, out);
 }
 
-int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan) {
-  k_abserrmax<<<kRedBlocks, 256, 0, c->stream>>>(c->N, xn, xp, c->part);
+int abserrmax(msg_ctx *c, double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan,
+              const double *dh) {
+  k_abserrmax<<<kRedBlocks, 256, 0, c->stream>>>(c->N, xn, xp, dh, c->part);
   MSG_CHECK_LAUNCH();
   int rc = fetch_partials(c, kRedBlocks * 8);
   if (rc) return rc;
@@ -363,6 +365,56 @@ int abserrmax(msg_ctx *c, const double *xn, const double *xp, double *chmax, dou
   *nan = nn;
   if (!nn) { *chmax = cv; *xmax = xv; *nun = (int)ci + 1; }
   else { *chmax = 0.0; *xmax = NAN; *nun = 0; }
+  return MSG_OK;
+}
+
+// The line search's four reductions over the full step in one pass (run_backtr,
+// Nonlinear_solution.f90:441-512): ||dh||^2, ||F(h + dh)||^2, the slope (s, J dh) and
+// lam_length's largest ratio |dh| / |h|.  The sums use the grid and order of k_dot2, so each
+// has the bits of its own dot product; J dh is jv, or b - r (BiCGStab's residual from dh = 0)
+// formed with the rounding of the axpby it replaces.  The maximum is exact whatever the grid.
+__global__ void __launch_bounds__(256) k_backtr_stats(int n, const double *dh, const double *hn, const double *f,
+                                                      const double *s, const double *jv, const double *b,
+                                                      const double *r, double *part) {
+  __shared__ double sh[8];
+  __shared__ double sm[256];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, num = 1.0, den = 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = dh[i], fi = f[i];
+    s0 = __dadd_rn(s0, __dmul_rn(d, d));
+    s1 = __dadd_rn(s1, __dmul_rn(fi, fi));
+    const double j = jv ? jv[i] : __dadd_rn(b[i], __dmul_rn(-1.0, r[i]));
+    s2 = __dadd_rn(s2, __dmul_rn(s[i], j));
+    const double h = fabs(hn[i]), a = fabs(d);
+    if (h != 0.0 && ratio_greater(a, h, num, den)) { num = a; den = h; }
+  }
+  double t = block_sum<256>(s0, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  t = block_sum<256>(s1, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = t;
+  t = block_sum<256>(s2, sh);
+  if (threadIdx.x == 0) part[2 * gridDim.x + blockIdx.x] = t;
+  sm[threadIdx.x] = __ddiv_rn(num, den);
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[3 * gridDim.x + blockIdx.x] = sm[0];
+}
+
+int backtr_stats(msg_ctx *c, const double *dh, const double *hn, const double *f, const double *s, const double *jv,
+                 const double *b, const double *r, double out[4]) {
+  const int nb = nblk(c->N);
+  if ((size_t)4 * nb > c->npart) { set_error("backtr_stats: partials buffer too small"); return MSG_ERR_STATE; }
+  k_backtr_stats<<<nb, 256, 0, c->stream>>>(c->N, dh, hn, f, s, jv, b, r, c->part);
+  MSG_CHECK_LAUNCH();
+  k_finish<8><<<4, 1024, 0, c->stream>>>(c->part, nb, c->dres);
+  MSG_CHECK_LAUNCH();
+  MSG_CUDA(cudaMemcpyAsync(c->hpin, c->dres, 32, cudaMemcpyDeviceToHost, c->stream));
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; ++k) out[k] = c->hpin[k];
+  out[3] = std::fmax(1.0, c->hpin[3]);
   return MSG_OK;
 }
 
@@ -539,12 +591,16 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
   double red[2];
   double sk = 0.0, sk0 = 1.0e20, sk2, alpha = 0.0, beta, omega = 1.0, ts, tt;
   bool need_dilu = (c->prm.precon_type == 0) || c->prm.ref_quirks;
+  // r* (fixed during the solve), the first search direction and the residual before the
+  // first update.  From x = 0 all three are b itself: nothing is copied, and x is first
+  // written (not read) by the first update.
+  const double *rs, *p1, *r1;
   if (x_zero) {
-    // x = 0 (the Newton correction starts from zero): r = r* = p = b, sk = <b, b>
     if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
-    k_bicg_start0<<<nb, 256, 0, c->stream>>>(n, c->rhs, c->r, c->rs, c->p, c->part);
+    k_dot2<<<nb, 256, 0, c->stream>>>(n, c->rhs, c->rhs, nullptr, c->part);   // sk = <b, b>
     MSG_CHECK_LAUNCH();
     if ((rc = finish(c, nb, 1, &sk))) return rc;
+    rs = p1 = r1 = c->rhs;
   } else {
     // r = b - A x
     k_spmv<0, true><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, x, c->rhs, c->r, nullptr, nullptr);
@@ -552,23 +608,28 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
     if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
     MSG_CUDA(cudaMemcpyAsync(c->rs, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = dot(c, c->r, c->rs, n, &sk))) return rc;
+    rs = p1 = c->rs;
+    r1 = c->r;
   }
   c->conv_flag = 0;
   for (c->in_iter = 1; c->in_iter <= c->prm.maxinn_iter; ++c->in_iter) {
+    const double *p = c->p;
     if (c->in_iter == 1) {
-      if (!x_zero) MSG_CUDA(cudaMemcpyAsync(c->p, c->r, (size_t)n * 8, cudaMemcpyDeviceToDevice, c->stream));
+      p = p1;
     } else {
       beta = (sk / sk0) * (alpha / omega);
-      k_bicg_p<<<nb, 256, 0, c->stream>>>(n, c->p, c->r, c->v, beta, omega);
+      k_bicg_p<<<nb, 256, 0, c->stream>>>(n, c->in_iter == 2 ? p1 : c->p, c->p, c->r, c->v, beta, omega);
       MSG_CHECK_LAUNCH();
     }
-    if ((rc = apply_prec(c, c->p, c->z))) return rc;
-    k_spmv<1, false><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->v, c->rs, c->part);
+    if ((rc = apply_prec(c, p, c->z))) return rc;
+    k_spmv<1, false><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->v, rs, c->part);
     MSG_CHECK_LAUNCH();
     if ((rc = finish(c, nb, 1, red))) return rc;
     sk2 = red[0];
     alpha = sk / sk2;
-    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, x, c->r, c->z, c->v, c->rs, alpha, c->part);
+    const bool first = (c->in_iter == 1);
+    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, first && x_zero ? nullptr : x, x, first ? r1 : c->r, c->r, c->z, c->v,
+                                        rs, alpha, c->part);
     MSG_CHECK_LAUNCH();
     if ((rc = finish(c, nb, 1, red))) return rc;
     c->rnorm = red[0];
@@ -581,7 +642,7 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
     ts = red[0];
     tt = red[1];
     omega = ts / tt;
-    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, x, c->r, c->z, c->t, c->rs, omega, c->part);
+    k_bicg_xr<<<nb, 256, 0, c->stream>>>(n, x, x, c->r, c->r, c->z, c->t, rs, omega, c->part);
     MSG_CHECK_LAUNCH();
     if ((rc = finish(c, nb, 2, red))) return rc;
     c->rnorm = red[0];
