@@ -99,9 +99,10 @@ static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse) {
   if (c->timing) cudaEventRecord(ev[0], c->stream);
   int rc = launch_make_matvec(c, reuse);
   if (rc) return rc;
-  double s = sum_part(c, flux_parts(c), &rc);
-  if (rc) return rc;
-  if (l2_rhs) *l2_rhs = s;
+  if (l2_rhs) {   // ||F||^2 (a host round trip; calc_numsol needs it at its first iteration only)
+    *l2_rhs = sum_part(c, flux_parts(c), &rc);
+    if (rc) return rc;
+  }
   if (c->timing) cudaEventRecord(ev[1], c->stream);
   if (c->prm.precon_type == 1 && !c->prm.ref_quirks) {
     // amg_lag = k >= 1: the hierarchy built at a time step's first Newton iteration is
@@ -196,15 +197,24 @@ static int run_backtr(msg_ctx *c) {
   // r = rhs - J dh, so the slope below is (rhs, rhs - r), formed in one pass
   const bool jv_resid = c->prm.jv_mode == 1 && !c->prm.ref_quirks;
   if (!jv_resid && (rc = vecjacf(c, c->head_pre, c->head_change, jacvec, c->rhs))) return rc;
-  double dummy;
-  if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
+  // F(head_new) and its norm in the flux pass's order (l2_last, what calc_numsol keeps), the
+  // norm collected with the statistics below in one host round trip (timed runs take it
+  // through func_norm, which records the residual's time)
+  if (c->timing) {
+    double dummy;
+    if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
+  } else {
+    if ((rc = launch_calc_func(c, c->head_new, c->new_f, true))) return rc;
+    if ((rc = finish_to(c, flux_parts(c), 1, 4))) return rc;
+  }
   // ||dh||^2, ||F(head_new)||^2, the slope and lam_length in one pass; lam_length is taken
   // again if dh is shortened (the slope, from J dh of the unshortened step, is scaled below)
   const double *srhs = slope_from_rhs(c) ? c->rhs : c->slope_rhs;   // or (Q2) the last preconditioner input
-  double stats[4];
+  double stats[5];
   if ((rc = backtr_stats(c, c->head_change, c->head_new, c->new_f, srhs, jv_resid ? nullptr : jacvec, c->rhs, c->r,
-                         stats)))
+                         stats, !c->timing)))
     return rc;
+  if (!c->timing) c->l2_last = stats[4];
   const double l2_pnorm = stats[0];
   c->l2_new = stats[1];
   double slope = stats[2];
@@ -359,13 +369,13 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
   for (c->out_iter = 1; c->out_iter <= c->prm.maxout_iter; ++c->out_iter) {
     if (c->out_iter > 1) c->l2_pre = c->l2_new;
     c->back_flag = 0; c->back_iter = 0; c->beta_iter = 0;
-    double l2r;
+    double l2r = 0.0;
     // from the second iteration on, the previous iteration ended with F evaluated at
     // head_new (line search or the closing evaluation), leaving S, kr and the storage
     // term there in srat_new / kr / sto
     // the first assembly reuses S, kr and the storage term when the guess selection left
     // them at head_new (the chosen guess was the last one evaluated)
-    if ((rc = make_matvec(c, &l2r, c->out_iter > 1 || c->vg_at_head))) return rc;
+    if ((rc = make_matvec(c, c->out_iter == 1 ? &l2r : nullptr, c->out_iter > 1 || c->vg_at_head))) return rc;
     c->vg_at_head = 0;
     if (!slope_from_rhs(c) && (rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
     if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }

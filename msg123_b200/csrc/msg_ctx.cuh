@@ -125,13 +125,15 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero = false);
 int dot(msg_ctx *c, const double *a, const double *b, int n, double *out);   // sync + host value
 // sum narr partial arrays (nparts each, consecutive in c->part) on the device; sync; host values
 int finish(msg_ctx *c, int nparts, int narr, double *out);
+int finish_to(msg_ctx *c, int nparts, int narr, int slot);   // into dres[slot..], no wait
+int fetch_res(msg_ctx *c, int count, double *out);           // dres[0..count) to the host (waits)
 int norm1(msg_ctx *c, const double *a, int n, double *out);
 int abserrmax(msg_ctx *c, double *xn, const double *xp, double *chmax, double *xmax, int *nun, int *nan,
               const double *dh = nullptr);   // dh: form xn = xp + dh first
 int lam_length(msg_ctx *c, const double *dh, const double *hn, double *out);
 // ||dh||^2, ||f||^2, (s, jv) (jv null: (s, b - r)) and lam_length(dh, hn) in one pass
 int backtr_stats(msg_ctx *c, const double *dh, const double *hn, const double *f, const double *s, const double *jv,
-                 const double *b, const double *r, double out[4]);
+                 const double *b, const double *r, double out[5], bool slot4);   // slot4: also dres[4] (pending)
 int axpby(msg_ctx *c, double *y, const double *x, double a, const double *w, int n);   // y = x + a*w
 int scale(msg_ctx *c, double *y, double a, int n);
 

@@ -325,13 +325,25 @@ __global__ void __launch_bounds__(1024) k_finish(const double *part, int nparts,
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
-int finish(msg_ctx *c, int nparts, int narr, double *out) {
-  k_finish<<<narr, 1024, 0, c->stream>>>(c->part, nparts, c->dres);
+// Second stage into dres[slot .. slot + narr) without waiting: results of several
+// reductions come back with one fetch_res (one host round trip).
+int finish_to(msg_ctx *c, int nparts, int narr, int slot) {
+  k_finish<<<narr, 1024, 0, c->stream>>>(c->part, nparts, c->dres + slot);
   MSG_CHECK_LAUNCH();
-  MSG_CUDA(cudaMemcpyAsync(c->hpin, c->dres, (size_t)narr * 8, cudaMemcpyDeviceToHost, c->stream));
-  MSG_CUDA(cudaStreamSynchronize(c->stream));
-  for (int a = 0; a < narr; ++a) out[a] = c->hpin[a];
   return MSG_OK;
+}
+
+int fetch_res(msg_ctx *c, int count, double *out) {
+  MSG_CUDA(cudaMemcpyAsync(c->hpin, c->dres, (size_t)count * 8, cudaMemcpyDeviceToHost, c->stream));
+  MSG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int a = 0; a < count; ++a) out[a] = c->hpin[a];
+  return MSG_OK;
+}
+
+int finish(msg_ctx *c, int nparts, int narr, double *out) {
+  int rc = finish_to(c, nparts, narr, 0);
+  if (rc) return rc;
+  return fetch_res(c, narr, out);
 }
 
 int dot(msg_ctx *c, const double *a, const double *b, int n, double *out) {
@@ -404,17 +416,16 @@ __global__ void __launch_bounds__(256) k_backtr_stats(int n, const double *dh, c
 }
 
 int backtr_stats(msg_ctx *c, const double *dh, const double *hn, const double *f, const double *s, const double *jv,
-                 const double *b, const double *r, double out[4]) {
+                 const double *b, const double *r, double out[5], bool slot4) {
   const int nb = nblk(c->N);
   if ((size_t)4 * nb > c->npart) { set_error("backtr_stats: partials buffer too small"); return MSG_ERR_STATE; }
   k_backtr_stats<<<nb, 256, 0, c->stream>>>(c->N, dh, hn, f, s, jv, b, r, c->part);
   MSG_CHECK_LAUNCH();
   k_finish<8><<<4, 1024, 0, c->stream>>>(c->part, nb, c->dres);
   MSG_CHECK_LAUNCH();
-  MSG_CUDA(cudaMemcpyAsync(c->hpin, c->dres, 32, cudaMemcpyDeviceToHost, c->stream));
-  MSG_CUDA(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < 3; ++k) out[k] = c->hpin[k];
-  out[3] = std::fmax(1.0, c->hpin[3]);
+  int rc = fetch_res(c, slot4 ? 5 : 4, out);
+  if (rc) return rc;
+  out[3] = std::fmax(1.0, out[3]);
   return MSG_OK;
 }
 
@@ -597,9 +608,10 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
   const double *rs, *p1, *r1;
   if (x_zero) {
     if (need_dilu && (rc = launch_precon_dilu(c))) return rc;
-    k_dot2<<<nb, 256, 0, c->stream>>>(n, c->rhs, c->rhs, nullptr, c->part);   // sk = <b, b>
+    // sk = <b, b>, collected with the first (v, r*) in one host round trip
+    k_dot2<<<nb, 256, 0, c->stream>>>(n, c->rhs, c->rhs, nullptr, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = finish(c, nb, 1, &sk))) return rc;
+    if ((rc = finish_to(c, nb, 1, 2))) return rc;
     rs = p1 = r1 = c->rhs;
   } else {
     // r = b - A x
@@ -624,7 +636,14 @@ int solve_bicgs(msg_ctx *c, double *x, bool x_zero) {
     if ((rc = apply_prec(c, p, c->z))) return rc;
     k_spmv<1, false><<<nb, 256, 0, c->stream>>>(g, c->dmat, c->lu, c->z, nullptr, c->v, rs, c->part);
     MSG_CHECK_LAUNCH();
-    if ((rc = finish(c, nb, 1, red))) return rc;
+    if (x_zero && c->in_iter == 1) {
+      double got[3];
+      if ((rc = finish_to(c, nb, 1, 0)) || (rc = fetch_res(c, 3, got))) return rc;
+      red[0] = got[0];
+      sk = got[2];
+    } else if ((rc = finish(c, nb, 1, red))) {
+      return rc;
+    }
     sk2 = red[0];
     alpha = sk / sk2;
     const bool first = (c->in_iter == 1);
