@@ -94,10 +94,12 @@ static int func_norm(msg_ctx *c, const double *h, double *F, double *l2) {
 
 // make_matvec (Make_linearsystem.f90:24-68) + AMG setup when requested.  reuse: the last
 // residual evaluation was at head_new (true from the second Newton iteration on).
-static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse) {
+// assembled: the line search already assembled the system at head_new (asm_ahead), so only
+// the hierarchy decision remains.
+static int make_matvec(msg_ctx *c, double *l2_rhs, bool reuse, bool assembled = false) {
   cudaEvent_t *ev = c->ev;
   if (c->timing) cudaEventRecord(ev[0], c->stream);
-  int rc = launch_make_matvec(c, reuse);
+  int rc = assembled ? MSG_OK : launch_make_matvec(c, reuse);
   if (rc) return rc;
   if (l2_rhs) {   // ||F||^2 (a host round trip; calc_numsol needs it at its first iteration only)
     *l2_rhs = sum_part(c, flux_parts(c), &rc);
@@ -171,6 +173,7 @@ static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out, co
 }
 
 static int calc_funcl2norm(msg_ctx *c, double in_lam) {
+  c->asm_ahead = 0;   // head_new moves off the point the system was assembled at
   int rc = axpby(c, c->head_new, c->head_pre, in_lam, c->head_change, c->N);
   if (rc) return rc;
   return func_norm(c, c->head_new, c->new_f, &c->l2_new);
@@ -200,9 +203,25 @@ static int run_backtr(msg_ctx *c) {
   // F(head_new) and its norm in the flux pass's order (l2_last, what calc_numsol keeps), the
   // norm collected with the statistics below in one host round trip (timed runs take it
   // through func_norm, which records the residual's time)
+  //
+  // Assembly ahead: unless the line search backtracks, the next Newton iteration assembles
+  // the system at this same head_new, and the assembly pass computes F(head_new) (as -F in
+  // its right-hand side, term for term the residual pass's arithmetic, with the same F^2
+  // partials) and S, kr and the storage term there.  So the residual evaluation at the
+  // full step is the assembly itself, into rhs_alt (the current rhs is still needed for the
+  // slope): one van Genuchten and one flux pass per Newton iteration fewer.  Not with the
+  // convergence log (it records this iteration's dmat), the phase timers or the reference's
+  // quirks.
+  const bool ahead = !c->timing && !c->clog_on && !c->prm.ref_quirks;
+  const double *fnew = c->new_f;
   if (c->timing) {
     double dummy;
     if ((rc = func_norm(c, c->head_new, c->new_f, &dummy))) return rc;
+  } else if (ahead) {
+    if ((rc = launch_make_matvec(c, false, c->rhs_alt))) return rc;
+    if ((rc = finish_to(c, flux_parts(c), 1, 4))) return rc;
+    fnew = c->rhs_alt;   // -F: the same squares
+    c->asm_ahead = 1;
   } else {
     if ((rc = launch_calc_func(c, c->head_new, c->new_f, true))) return rc;
     if ((rc = finish_to(c, flux_parts(c), 1, 4))) return rc;
@@ -211,7 +230,7 @@ static int run_backtr(msg_ctx *c) {
   // again if dh is shortened (the slope, from J dh of the unshortened step, is scaled below)
   const double *srhs = slope_from_rhs(c) ? c->rhs : c->slope_rhs;   // or (Q2) the last preconditioner input
   double stats[5];
-  if ((rc = backtr_stats(c, c->head_change, c->head_new, c->new_f, srhs, jv_resid ? nullptr : jacvec, c->rhs, c->r,
+  if ((rc = backtr_stats(c, c->head_change, c->head_new, fnew, srhs, jv_resid ? nullptr : jacvec, c->rhs, c->r,
                          stats, !c->timing)))
     return rc;
   if (!c->timing) c->l2_last = stats[4];
@@ -363,6 +382,7 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
   memset(&st, 0, sizeof(st));
   double l2x;
   c->amg_age++;
+  c->asm_ahead = 0;
   if ((rc = dot(c, c->head_new, c->head_new, n, &l2x))) return rc;      // set_backtr
   c->maxstep = std::sqrt(l2x) * VARMAX;
   if (c->maxstep < 1.0) c->maxstep = 1.0;
@@ -375,7 +395,15 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     // term there in srat_new / kr / sto
     // the first assembly reuses S, kr and the storage term when the guess selection left
     // them at head_new (the chosen guess was the last one evaluated)
-    if ((rc = make_matvec(c, c->out_iter == 1 ? &l2r : nullptr, c->out_iter > 1 || c->vg_at_head))) return rc;
+    // the previous iteration's line search assembled the system at head_new (its rhs is in
+    // rhs_alt) unless it backtracked
+    const bool assembled = c->asm_ahead;
+    if (assembled) {
+      std::swap(c->rhs, c->rhs_alt);
+      c->asm_ahead = 0;
+    }
+    if ((rc = make_matvec(c, c->out_iter == 1 ? &l2r : nullptr, c->out_iter > 1 || c->vg_at_head, assembled)))
+      return rc;
     c->vg_at_head = 0;
     if (!slope_from_rhs(c) && (rc = copy_d2d(c, c->slope_rhs, c->rhs, n))) return rc;
     if (c->out_iter == 1) { c->l2_new = l2r; c->l2_pre = c->l2_new; c->eta = 0.5; }
@@ -623,7 +651,7 @@ static int create_impl(msg_ctx *c, const msg_grid_t *g, const msg_params_t *p) {
   ALLOC(c->offind, (N + 1) * 4);
   double **vn[] = {&c->head_new, &c->head_old, &c->head_old2, &c->head_pre, &c->head_change, &c->srat_new, &c->srat_old,
                    &c->new_f, &c->kr, &c->kr_per, &c->alp, &c->sto, &c->stod, &c->tmpv, &c->dmat, &c->rhs,
-                   &c->slope_rhs, &c->dilu_d, &c->r, &c->rs, &c->p, &c->v, &c->t, &c->z};
+                   &c->slope_rhs, &c->rhs_alt, &c->dilu_d, &c->r, &c->rs, &c->p, &c->v, &c->t, &c->z};
   for (auto q : vn) { ALLOC(*q, N * 8); MSG_CUDA(cudaMemsetAsync(*q, 0, N * 8, c->stream)); }
   ALLOC(c->lu, 6 * N * 8);
   if (p->precision == 1) {
@@ -1232,7 +1260,7 @@ static void free_ctx(msg_ctx *c) {
                 c->rech_base, c->sea_hydf, c->sea_abyd, c->read_seal, c->drain, c->offind, c->offrow, c->conn_dir,
                 c->left_off, c->right_off, c->hydf_conn, c->abyd_conn, c->head_new, c->head_old, c->head_pre,
                 c->head_change, c->srat_new, c->srat_old, c->surf_head, c->surf_old, c->new_f, c->kr, c->kr_per,
-                c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->head_old2, c->slope_rhs, c->dilu_d, c->r, c->rs,
+                c->alp, c->sto, c->stod, c->tmpv, c->dmat, c->lu, c->rhs, c->rhs_alt, c->head_old2, c->slope_rhs, c->dilu_d, c->r, c->rs,
                 c->p, c->v, c->t, c->z, c->part, c->plane_ptr, c->plane_cells, c->dmat_f, c->lu_f, c->dres};
   for (auto q : dp) if (q) cudaFree(q);
   if (c->hpin) cudaFreeHost(c->hpin);

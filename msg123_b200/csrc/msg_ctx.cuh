@@ -54,6 +54,7 @@ struct msg_ctx {
   double *tmpv;                                  // [N] spare vector (J.v, line search)
   // ---- level-1 system, DIA: lu[d*N + i] = J(i, nb_d(i)) --------------------------------
   double *dmat, *lu, *rhs, *slope_rhs;
+  double *rhs_alt;                               // rhs assembled ahead by the line search (asm_ahead)
   float *dmat_f, *lu_f;                          // FP32 images (precision = 1)
   // ---- Krylov work ----------------------------------------------------------------------
   double *dilu_d, *r, *rs, *p, *v, *t, *z;
@@ -80,6 +81,7 @@ struct msg_ctx {
   int guess_rejected;                            // learned guesses not used (larger residual)
   int guess_skip, guess_backoff;                 // guess_select 2: steps left without the network, next pause
   int vg_at_head;                                // S, kr, storage in memory are those of head_new (reuse)
+  int asm_ahead;                                 // dmat, lu, rhs_alt: the system assembled at head_new
   // convergence log (msg_gpu_set_convlog): records of the Newton iterations, oldest first
   void *clog;                                    // std::deque<msg_convrec_t> (msg_api.cu)
   int clog_on;
@@ -104,7 +106,7 @@ int launch_water_table(msg_ctx *c, double *wt);
 int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm);
 // make_matvec at c->head_new: dmat, lu (DIA), rhs = -F.  reuse: srat_new, kr and sto
 // already hold the values at head_new (the last calc_func was evaluated there).
-int launch_make_matvec(msg_ctx *c, bool reuse = false);
+int launch_make_matvec(msg_ctx *c, bool reuse = false, double *rhs_out = nullptr);   // rhs_out null: c->rhs
 // Export the DIA Jacobian into the reference CSR order.
 int launch_dia_to_csr(msg_ctx *c, double *lumat_dev);
 int launch_mass(msg_ctx *c, double *out9_dev);

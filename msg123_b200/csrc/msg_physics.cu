@@ -756,14 +756,14 @@ int launch_calc_func(msg_ctx *c, const double *h, double *F, bool norm) {
   return MSG_OK;
 }
 
-int launch_make_matvec(msg_ctx *c, bool reuse) {
+int launch_make_matvec(msg_ctx *c, bool reuse, double *rhs_out) {
   const int bc = c->blk_cell > 0 ? c->blk_cell : kThreads;
   auto k = c->prm.vg_form ? (reuse ? k_cell<true, true, 1> : k_cell<true, false, 1>)
                            : (reuse ? k_cell<true, true, 0> : k_cell<true, false, 0>);
   k<<<(c->N + bc - 1) / bc, bc, 0, c->stream>>>(c->N, cell_args(c, c->head_new));
   MSG_CHECK_LAUNCH();
   FluxArgs a = flux_args(c, c->head_new);
-  a.F = c->rhs;
+  a.F = rhs_out ? rhs_out : c->rhs;
   a.dmat = c->dmat;
   a.lu = c->lu;
   a.dmat_f = c->dmat_f;
