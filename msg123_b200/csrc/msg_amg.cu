@@ -1366,7 +1366,10 @@ int amg_reserve(msg_ctx *c) {
   const size_t cap = (kArenaPerCell * (size_t)c->N + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
   if (cudaMalloc((void **)&A->arena, cap) == cudaSuccess) A->arena_cap = cap;
   else { A->arena = nullptr; A->arena_cap = 0; cudaGetLastError(); }   // the builds use the pool
-  return MSG_OK;
+  // and the setup scratch of the fine level (strength flags, MIS-2 state and tuples,
+  // temporaries: about 64 B per cell), which the first build would otherwise take from the
+  // pool: at 25.2M cells that first build then cost 20-45 ms more, varying from run to run
+  return ensure_scratch(c, A, (size_t)c->N, (size_t)c->nnz);
 }
 
 static int amg_state(msg_ctx *c) {

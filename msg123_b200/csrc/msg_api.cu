@@ -174,6 +174,7 @@ static int vecjacf(msg_ctx *c, const double *x, const double *v, double *out, co
 
 static int calc_funcl2norm(msg_ctx *c, double in_lam) {
   c->asm_ahead = 0;   // head_new moves off the point the system was assembled at
+  c->head_moved = 1;
   int rc = axpby(c, c->head_new, c->head_pre, in_lam, c->head_change, c->N);
   if (rc) return rc;
   return func_norm(c, c->head_new, c->new_f, &c->l2_new);
@@ -418,6 +419,8 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     st.inner_total += c->in_iter; st.in_iter_last = c->in_iter;
     // head_new = head_pre + dh, formed inside check_abserrmax's pass
     if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan, c->head_change))) return rc;
+    const double maxvar_full = c->maxvar, maxunk_full = maxunk;   // of the full step, for the line search below
+    const int maxnun_full = maxnun, nan_full = nan;
     check_val = std::fabs(c->maxvar) * c->len_scal;
     maxunk = std::fabs(maxunk) * c->len_scal;
     double crit = c->prm.criteria_rel ? c->prm.criteria * maxunk : c->prm.criteria;
@@ -430,9 +433,15 @@ static int calc_numsol(msg_ctx *c, msg_stats_t *stx) {
     }
     bool evaluated = false;   // F(head_new) and its norm already computed by the line search
     if (c->conv_flag != 1) {
+      c->head_moved = 0;
       if ((rc = run_backtr(c))) return rc;
       evaluated = true;
-      if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
+      // check_abserrmax again: the same values as above unless the line search moved head_new
+      if (c->head_moved) {
+        if ((rc = abserrmax(c, c->head_new, c->head_pre, &c->maxvar, &maxunk, &maxnun, &nan))) return rc;
+      } else {
+        c->maxvar = maxvar_full; maxunk = maxunk_full; maxnun = maxnun_full; nan = nan_full;
+      }
       check_val = std::fabs(c->maxvar) * c->len_scal;
       maxunk = std::fabs(maxunk) * c->len_scal;
       crit = c->prm.criteria_rel ? c->prm.criteria * maxunk : c->prm.criteria;

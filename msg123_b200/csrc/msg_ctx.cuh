@@ -82,6 +82,7 @@ struct msg_ctx {
   int guess_skip, guess_backoff;                 // guess_select 2: steps left without the network, next pause
   int vg_at_head;                                // S, kr, storage in memory are those of head_new (reuse)
   int asm_ahead;                                 // dmat, lu, rhs_alt: the system assembled at head_new
+  int head_moved;                                // the line search moved head_new off the full step
   // convergence log (msg_gpu_set_convlog): records of the Newton iterations, oldest first
   void *clog;                                    // std::deque<msg_convrec_t> (msg_api.cu)
   int clog_on;
