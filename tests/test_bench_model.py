@@ -163,7 +163,10 @@ def test_bench_main_dry_run(monkeypatch, capsys, extra):
         assert k in line, k
     assert line["value"] == pytest.approx(256 * 2 / 10e-3)
     r = line["roofline"]
-    assert r["ms_per_launch"] == 0.02 and r["unit"] == "GB/s" and 0 < r["frac"]
+    # the assembly pair (make_matvec, kernel_time 2) is the line's dominant kernel; the others sit beside it
+    assert r["ms_per_launch"] == 0.03 and r["unit"] == "GB/s" and 0 < r["frac"]
+    assert r["alg_bytes_per_cell"] == 280.0 and r["traffic"] == pytest.approx((93.8 + 170.8) * 256)
+    assert r["others"]["calc_func (vG pass + flux pass)"]["ms"] == 0.02
     assert r["others"]["mixed V-cycle, all levels"]["ms"] == 0.05
     assert r["vcycle_mixed_ms"] == 0.05 and line["config"]["workload"].startswith("hetero 8x8x4")
     assert line["newton"]["accepted"] == 2 and line["newton"]["simulated_s"] == 3000.0 and line["window_start_s"] == 1800.0
