@@ -221,7 +221,12 @@ MSG_API int msg_gpu_vecjacf(msg_ctx_t *ctx, const double *x, const double *v, do
 MSG_API int msg_gpu_solve_linalg(msg_ctx_t *ctx, double init_norm, double errtol, double *inx,
                          double *last_norm, int32_t *in_iter, int32_t *conv_flag);
 
-/* calc_numsol (Nonlinear_solution.f90:33-294): one time level's Newton solve. */
+/* calc_numsol (Nonlinear_solution.f90:33-294): one time level's Newton solve.  Heads,
+ * statistics and the convergence log are those of the reference's loop.  Unless the
+ * convergence log, the phase timers or ref_quirks are on, the line search's residual
+ * evaluation at the full step is an assembly (used by the next Newton iteration), so on
+ * return the device's level-1 system may be the one assembled at the final head rather
+ * than at the last iteration's; msg_gpu_make_matvec re-assembles it at head_new. */
 MSG_API int msg_gpu_calc_numsol(msg_ctx_t *ctx, msg_stats_t *stats);
 
 /* Time loop (Msg.f90:83-104 with update_tstep/calc_nextst, Time_module.f90:34-273):
